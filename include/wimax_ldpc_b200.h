@@ -1,0 +1,203 @@
+/*
+ * wimax_ldpc_b200 -- C ABI of the B200-native WiMAX (IEEE 802.16e) QC-LDPC codec.
+ *
+ * The reference library (myersw12/wimax_ldpc_lib) exposes C++ classes only
+ * (reference include/ldpc_decoder.h, include/ldpc_encoder.h,
+ * include/BER_runner.h) and has no FFI of its own. This header is the flat
+ * boundary those classes map onto: one opaque handle per reference object,
+ * one entry point per public method, plain pointers and sizes, int status
+ * codes. The C++ facade in include/wimax_ldpc_lib/ re-creates the reference
+ * classes on top of it; a ctypes / cgo / JNI binding binds these symbols.
+ *
+ * Conventions (same as the reference):
+ *   rate   coderate enum: 0 = 1/2, 1 = 2/3A, 2 = 2/3B, 3 = 3/4A, 4 = 3/4B, 5 = 5/6
+ *          (reference include/enums.h:4-12)
+ *   z      expansion factor 24..96 step 4; n = 24*z (reference lib/ldpc.cc:15-16)
+ *   LLR    positive means bit 1; hard decision is x >= 0 (reference
+ *          lib/ldpc_decoder.cc:130,242; BPSK bit*2-1 in lib/BER_runner.cc:183)
+ *
+ * Every function returns WLDPC_OK (0) or a negative WLDPC_ERR_* code.
+ * Handles are not thread-safe (one per host thread), like the reference
+ * objects, which share per-object scratch (reference lib/ldpc_decoder.cc:36).
+ * The product path runs on the GPU only; without a CUDA device, calls that
+ * compute return WLDPC_ERR_NO_DEVICE.
+ */
+#ifndef WIMAX_LDPC_B200_H
+#define WIMAX_LDPC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define WLDPC_API __attribute__((visibility("default")))
+#else
+#define WLDPC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WLDPC_OK 0
+#define WLDPC_ERR_ARG (-1)          /* null / misaligned pointer, bad size or mode */
+#define WLDPC_ERR_CODE (-2)         /* invalid rate or z; the reference throws std::exception */
+#define WLDPC_ERR_CUDA (-3)         /* a CUDA runtime call or kernel launch failed */
+#define WLDPC_ERR_NO_DEVICE (-4)    /* no usable CUDA device */
+#define WLDPC_ERR_TIMEOUT (-5)      /* a bounded device-side wait expired */
+#define WLDPC_ERR_UNSUPPORTED (-6)  /* operation not available for this code */
+
+/* Decoder flavours: the reference's compile-time switch (reference
+ * lib/ldpc_decoder.cc:17-21), selectable at run time here. */
+#define WLDPC_MODE_NMS 0            /* normalized min-sum x0.815, as shipped */
+#define WLDPC_MODE_OMS 1            /* offset min-sum, offset 0.10 */
+#define WLDPC_MODE_MS 2             /* plain min-sum */
+
+WLDPC_API const char* wldpc_strerror(int code);
+/* ABI version: major * 10000 + minor * 100 + patch */
+WLDPC_API int wldpc_version(void);
+
+/* ------------------------------------------------------------ code tables */
+
+typedef struct wldpc_code_info {
+    int rate, z;
+    int n;        /* codeword bits, reference m_N (lib/ldpc.cc:16) */
+    int m;        /* parity bits, reference m_M (lib/ldpc.cc:18-44) */
+    int k;        /* info bits, n - m */
+    int rows;     /* expanded check rows, reference m_row_size */
+    int cols;     /* max row degree, reference m_col_size */
+    int D, X;     /* encoder constants, reference m_D / m_X */
+    int layers;   /* base rows */
+    int edges;    /* non-zero entries of H */
+} wldpc_code_info;
+
+/* Replaces ldpc::ldpc(rate, z, threads) + set_checknode_array (reference
+ * lib/ldpc.cc:11-62,69-1206): WLDPC_ERR_CODE where the reference throws. */
+WLDPC_API int wldpc_code_info_get(int rate, unsigned z, wldpc_code_info* out);
+
+/* The expanded check-node table in the reference's layout: int16
+ * [rows][cols], -1 padded (reference lib/matrices/wimax_N_RATE.cc).
+ * capacity is in elements. */
+WLDPC_API int wldpc_checknode_table(int rate, unsigned z, int16_t* out, size_t capacity);
+
+/* ---------------------------------------------------------------- decoder */
+
+typedef struct wldpc_decoder wldpc_decoder;
+
+/* Replaces ldpc_decoder::ldpc_decoder(rate, z, max_iter, num_threads)
+ * (reference include/ldpc_decoder.h:25-28, lib/ldpc_decoder.cc:27-59).
+ * num_threads is kept for signature parity and unused, as in the reference.
+ * mode is WLDPC_MODE_*; the reference build is WLDPC_MODE_NMS. */
+WLDPC_API int wldpc_decoder_create(int rate, unsigned z, unsigned max_iter, unsigned num_threads, int mode,
+                         wldpc_decoder** out);
+/* Replaces ldpc_decoder::~ldpc_decoder (reference lib/ldpc_decoder.cc:61-65). */
+WLDPC_API int wldpc_decoder_destroy(wldpc_decoder* dec);
+
+/* Replaces unsigned ldpc_decoder::decode(float* rx_codeword, int8_t* decoded)
+ * (reference include/ldpc_decoder.h:33, lib/ldpc_decoder.cc:122-262). Host
+ * pointers. rx_codeword (n floats) is overwritten with the posterior LLRs and
+ * decoded receives n bytes 0/1, exactly as the reference. *num_errors gets the
+ * reference's return value: 0 when the syndrome is satisfied (and always 0
+ * when max_iter == 0), 1 otherwise. *iterations (nullable) receives the
+ * iterations executed, which the reference does not report. Synchronous. */
+WLDPC_API int wldpc_decoder_decode(wldpc_decoder* dec, float* rx_codeword, int8_t* decoded, unsigned* num_errors,
+                         int* iterations);
+
+/* Replaces unsigned ldpc_decoder::decode(int8_t* rx_codeword, int8_t* decoded)
+ * (reference include/ldpc_decoder.h:32, lib/ldpc_decoder.cc:108-118): the
+ * bytes are mapped to bit*2.0-1.0 and decoded; the input is not modified. */
+WLDPC_API int wldpc_decoder_decode_bits(wldpc_decoder* dec, const int8_t* rx_codeword, int8_t* decoded,
+                              unsigned* num_errors);
+
+/* Replaces unsigned ldpc_decoder::compute_syndrome(int8_t*, bool)
+ * (reference include/ldpc_decoder.h:31, lib/ldpc_decoder.cc:67-104): number
+ * of failing check rows (row parity is the XOR of the bytes), or 0/1 when
+ * exit_early is non-zero. */
+WLDPC_API int wldpc_decoder_compute_syndrome(wldpc_decoder* dec, const int8_t* rx_codeword, int exit_early,
+                                   unsigned* num_errors);
+
+/* Batched decode on device memory, asynchronous on `stream` (a cudaStream_t;
+ * NULL is the CUDA default stream). The batch form of decode(float*, int8_t*):
+ *   llr       frames x n float32, 16-byte aligned
+ *   decoded   frames x n int8 (0/1), 4-byte aligned
+ *   posterior frames x n float32 or NULL, 16-byte aligned; may equal llr
+ *             (in-place posterior, the reference's semantics)
+ *   status    frames int32 or NULL: iterations | (syndrome_failed << 16)
+ * The reference return value of frame f is (max_iter == 0) ? 0 : status>>16. */
+WLDPC_API int wldpc_decode_batch_device(wldpc_decoder* dec, const float* llr, int8_t* decoded, float* posterior,
+                              int32_t* status, size_t frames, void* stream);
+
+/* Batched decode of host buffers (pinned or pageable), synchronous, with the
+ * host<->device copies pipelined against the kernels. rx_codewords is
+ * overwritten with the posterior (reference semantics); num_errors and
+ * status are nullable (frames entries each). */
+WLDPC_API int wldpc_decode_batch_host(wldpc_decoder* dec, float* rx_codewords, int8_t* decoded, uint32_t* num_errors,
+                            int32_t* status, size_t frames);
+
+/* Waits for the device and reports a device-side error (WLDPC_ERR_TIMEOUT)
+ * recorded by earlier launches of this decoder. */
+WLDPC_API int wldpc_decoder_synchronize(wldpc_decoder* dec);
+
+/* ---------------------------------------------------------------- encoder */
+
+typedef struct wldpc_encoder wldpc_encoder;
+
+/* Replaces ldpc_encoder::ldpc_encoder(rate, z, num_threads) (reference
+ * include/ldpc_encoder.h:21, lib/ldpc_encoder.cc:9-17). Like the reference
+ * class, rate 3/4B is accepted; its output is whatever the dual-diagonal
+ * recursion yields (the reference's tools refuse 3/4B, README.md:25). */
+WLDPC_API int wldpc_encoder_create(int rate, unsigned z, unsigned num_threads, wldpc_encoder** out);
+WLDPC_API int wldpc_encoder_destroy(wldpc_encoder* enc);
+
+/* Replaces void ldpc_encoder::encode_data(uint8_t* infoword, uint8_t* codeword)
+ * (reference include/ldpc_encoder.h:24, lib/ldpc_encoder.cc:50-105): k input
+ * bytes (non-zero = 1), n output bytes, systematic part copied verbatim. */
+WLDPC_API int wldpc_encoder_encode(wldpc_encoder* enc, const uint8_t* infoword, uint8_t* codeword);
+
+/* Batched encode on device memory (frames x k in, frames x n out, both
+ * 4-byte aligned), asynchronous on stream (NULL = the CUDA default stream). */
+WLDPC_API int wldpc_encode_batch_device(wldpc_encoder* enc, const uint8_t* info, uint8_t* codeword, size_t frames,
+                              void* stream);
+
+/* --------------------------------------------------------- frame generator */
+
+/* Seeded synthetic frames on device (the GPU stand-in for BER_runner's frame
+ * generation, reference lib/BER_runner.cc:162-191): info bits from Philox4x32-10
+ * (key = seed, counter = (block, frame, stream)), the encoder above, BPSK
+ * bit*2-1, AWGN with sigma^2 = 1/(2 R Eb/N0), LLR = 2y/sigma^2 (positive = 1).
+ * Eb/N0 in dB is drawn per frame uniformly in [ebno_lo_db, ebno_hi_db].
+ * first_frame offsets the frame counter so that shards of one job draw
+ * disjoint frames. Any of info (frames x k), codeword (frames x n), llr
+ * (frames x n, 16-byte aligned) and ebno_db (frames) may be NULL. Rate 3/4B
+ * has no encoder and returns WLDPC_ERR_UNSUPPORTED. Asynchronous on stream. */
+WLDPC_API int wldpc_framegen_device(int rate, unsigned z, uint64_t seed, uint64_t first_frame, size_t frames,
+                          float ebno_lo_db, float ebno_hi_db, uint8_t* info, uint8_t* codeword, float* llr,
+                          float* ebno_db, void* stream);
+
+/* ------------------------------------------------------------- BER runner */
+
+typedef struct wldpc_ber_runner wldpc_ber_runner;
+
+/* Replaces BER_runner::BER_runner(rate, z, num_threads, max_iter) (reference
+ * include/BER_runner.h:53-57, lib/BER_runner.cc:15-87): 3/4B returns
+ * WLDPC_ERR_UNSUPPORTED where the reference throws. */
+WLDPC_API int wldpc_ber_runner_create(int rate, unsigned z, unsigned num_threads, unsigned max_iter,
+                            wldpc_ber_runner** out);
+WLDPC_API int wldpc_ber_runner_destroy(wldpc_ber_runner* b);
+/* Replaces double BER_runner::run_iteration(double EbNo_dB) (reference
+ * lib/BER_runner.cc:162-204): one frame with the reference's LFSR info bits,
+ * mt19937(0) / normal_distribution<float> noise stream and error count (over
+ * all n codeword bits, k added to the bit count); encode and decode run on
+ * the GPU. *ber gets the running errors / bits. */
+WLDPC_API int wldpc_ber_runner_run_iteration(wldpc_ber_runner* b, double ebno_db, double* ber);
+/* Replaces BER_runner::reset_test (reference lib/BER_runner.cc:96-102). */
+WLDPC_API int wldpc_ber_runner_reset(wldpc_ber_runner* b);
+/* Replaces get_total_num_bits / get_total_num_errors (reference :104-112). */
+WLDPC_API int wldpc_ber_runner_totals(wldpc_ber_runner* b, uint64_t* num_bits, uint64_t* num_errors);
+/* Replaces get_codeword_len / get_dataword_len (reference :114-122). */
+WLDPC_API int wldpc_ber_runner_lengths(wldpc_ber_runner* b, unsigned* codeword_len, unsigned* dataword_len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,55 @@
+"""GPU encoder and frame generator parity through the C ABI."""
+import numpy as np
+import pytest
+
+import inputs
+
+pytestmark = pytest.mark.gpu
+
+
+def test_encoder_golden_device_batch(wl, cuda, golden_encode):
+    torch = cuda
+    for c in golden_encode["cases"]:
+        n, m, k = inputs.code_dims(c["rate"], c["z"])
+        u = inputs.info_bits(c["seed"], c["frames"], k)
+        u[0, :4] = [2, 5, 255, 1]
+        enc = wl.Encoder(c["rate"], c["z"])
+        ud = torch.from_numpy(u).cuda()
+        cw = torch.empty((c["frames"], n), dtype=torch.uint8, device="cuda")
+        enc.encode_device(ud, cw)
+        torch.cuda.synchronize()
+        cw = cw.cpu().numpy()
+        assert [inputs.digest(cw[f]) for f in range(c["frames"])] == c["digests"], (c["rate"], c["z"])
+        assert inputs.digest(enc.encode(u[1])) == c["digests"][1]
+
+
+def test_encoder_large_batch_against_oracle(wl, cuda, oracle):
+    torch = cuda
+    for rate, z in [(0, 96), (5, 96), (2, 28), (3, 44)]:
+        n, m, k = inputs.code_dims(rate, z)
+        u = inputs.info_bits(rate + z, 4096, k)
+        cw = torch.empty((4096, n), dtype=torch.uint8, device="cuda")
+        wl.Encoder(rate, z).encode_device(torch.from_numpy(u).cuda(), cw)
+        torch.cuda.synchronize()
+        assert (cw.cpu().numpy() == oracle.encode(rate, z, u)).all()
+
+
+@pytest.mark.parametrize("rate", [0, 1, 2, 3, 5])
+def test_framegen_matches_oracle(wl, cuda, oracle, rate):
+    torch = cuda
+    for z in (24, 60, 96):
+        n, m, k = inputs.code_dims(rate, z)
+        frames = 64
+        info = torch.empty((frames, k), dtype=torch.uint8, device="cuda")
+        cw = torch.empty((frames, n), dtype=torch.uint8, device="cuda")
+        llr = torch.empty((frames, n), dtype=torch.float32, device="cuda")
+        eb = torch.empty(frames, dtype=torch.float32, device="cuda")
+        wl.framegen_device(rate, z, 99, 1000, frames, 1.0, 4.0, info, cw, llr, eb)
+        torch.cuda.synchronize()
+        oi, oc, ol, oe = oracle.framegen(rate, z, 99, 1000, frames, 1.0, 4.0)
+        assert (info.cpu().numpy() == oi).all() and (cw.cpu().numpy() == oc).all()
+        assert np.array_equal(eb.cpu().numpy(), oe.astype(np.float32))
+        # float transcendental functions on the GPU vs double on the host
+        l = llr.cpu().numpy().astype(np.float64)
+        tol = 2e-5 * np.maximum(1.0, np.abs(ol)) + 1e-4
+        assert (np.abs(l - ol) <= tol).all()

@@ -1,0 +1,284 @@
+"""wimax_ldpc_lib_b200 -- Python bindings of the B200-native WiMAX QC-LDPC codec.
+
+The product is ``lib/libwimax_ldpc_b200.so``: sm_100a kernels behind the C ABI
+declared in ``include/wimax_ldpc_b200.h`` plus the C++ facade of the
+reference's classes (``include/wimax_ldpc_lib/``). This module binds the C ABI
+with ctypes so that tests and ``bench.py`` can drive it; torch is used only to
+hold device memory and streams. There is no CPU fallback: if the shared library
+is missing, importing the bindings raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libwimax_ldpc_b200.so")
+INCLUDE_DIR = os.path.join(os.path.dirname(HERE), "include")
+
+HALFRATE, TWOTHIRDSA, TWOTHIRDSB, THREEQUARTERSA, THREEQUARTERSB, FIVESIXTHS = range(6)
+RATE_NAMES = ["1/2", "2/3A", "2/3B", "3/4A", "3/4B", "5/6"]
+Z_VALUES = tuple(range(24, 97, 4))
+MODE_NMS, MODE_OMS, MODE_MS = 0, 1, 2
+
+OK = 0
+ERR_ARG, ERR_CODE, ERR_CUDA, ERR_NO_DEVICE, ERR_TIMEOUT, ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6
+
+_p = ctypes.c_void_p
+_i = ctypes.c_int
+_u = ctypes.c_uint
+_sz = ctypes.c_size_t
+
+
+class LdpcError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        msg = _lib().wldpc_strerror(code).decode() if _LIB is not None else str(code)
+        super().__init__(f"{what}: {msg} ({code})" if what else f"{msg} ({code})")
+
+
+class CodeInfo(ctypes.Structure):
+    _fields_ = [("rate", _i), ("z", _i), ("n", _i), ("m", _i), ("k", _i), ("rows", _i), ("cols", _i),
+                ("D", _i), ("X", _i), ("layers", _i), ("edges", _i)]
+
+
+_LIB = None
+
+
+def build(jobs: int = 8) -> None:
+    """Compile lib/libwimax_ldpc_b200.so with nvcc (sm_100a); no GPU needed."""
+    import subprocess
+    subprocess.check_call(["make", "-s", "-C", HERE, f"-j{jobs}"])
+
+
+def _lib():
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run wimax_ldpc_lib_b200.build() (make -C wimax_ldpc_lib_b200)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.wldpc_strerror.restype = ctypes.c_char_p
+    L.wldpc_strerror.argtypes = [_i]
+    L.wldpc_version.argtypes = []
+    L.wldpc_code_info_get.argtypes = [_i, _u, ctypes.POINTER(CodeInfo)]
+    L.wldpc_checknode_table.argtypes = [_i, _u, _p, _sz]
+    L.wldpc_decoder_create.argtypes = [_i, _u, _u, _u, _i, ctypes.POINTER(_p)]
+    L.wldpc_decoder_destroy.argtypes = [_p]
+    L.wldpc_decoder_decode.argtypes = [_p, _p, _p, ctypes.POINTER(_u), ctypes.POINTER(_i)]
+    L.wldpc_decoder_decode_bits.argtypes = [_p, _p, _p, ctypes.POINTER(_u)]
+    L.wldpc_decoder_compute_syndrome.argtypes = [_p, _p, _i, ctypes.POINTER(_u)]
+    L.wldpc_decode_batch_device.argtypes = [_p, _p, _p, _p, _p, _sz, _p]
+    L.wldpc_decode_batch_host.argtypes = [_p, _p, _p, _p, _p, _sz]
+    L.wldpc_decoder_synchronize.argtypes = [_p]
+    L.wldpc_encoder_create.argtypes = [_i, _u, _u, ctypes.POINTER(_p)]
+    L.wldpc_encoder_destroy.argtypes = [_p]
+    L.wldpc_encoder_encode.argtypes = [_p, _p, _p]
+    L.wldpc_encode_batch_device.argtypes = [_p, _p, _p, _sz, _p]
+    L.wldpc_framegen_device.argtypes = [_i, _u, ctypes.c_uint64, ctypes.c_uint64, _sz, ctypes.c_float,
+                                        ctypes.c_float, _p, _p, _p, _p, _p]
+    L.wldpc_ber_runner_create.argtypes = [_i, _u, _u, _u, ctypes.POINTER(_p)]
+    L.wldpc_ber_runner_destroy.argtypes = [_p]
+    L.wldpc_ber_runner_run_iteration.argtypes = [_p, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
+    L.wldpc_ber_runner_reset.argtypes = [_p]
+    L.wldpc_ber_runner_totals.argtypes = [_p, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    L.wldpc_ber_runner_lengths.argtypes = [_p, ctypes.POINTER(_u), ctypes.POINTER(_u)]
+    _LIB = L
+    return L
+
+
+def lib():
+    """The loaded ctypes library (raises ImportError if it is not built)."""
+    return _lib()
+
+
+def _check(rc: int, what: str = "") -> None:
+    if rc != OK:
+        raise LdpcError(rc, what)
+
+
+def _np_ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _t_ptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def code_info(rate: int, z: int) -> CodeInfo:
+    ci = CodeInfo()
+    _check(_lib().wldpc_code_info_get(rate, z, ctypes.byref(ci)), "code_info")
+    return ci
+
+
+def checknode_table(rate: int, z: int) -> np.ndarray:
+    ci = code_info(rate, z)
+    t = np.empty(ci.rows * ci.cols, np.int16)
+    _check(_lib().wldpc_checknode_table(rate, z, _np_ptr(t), t.size), "checknode_table")
+    return t.reshape(ci.rows, ci.cols)
+
+
+def reference_return(status: np.ndarray, max_iter: int) -> np.ndarray:
+    """ldpc_decoder::decode's return value from a status word array."""
+    s = np.asarray(status)
+    return np.zeros(s.shape, np.uint32) if max_iter == 0 else ((s >> 16) & 1).astype(np.uint32)
+
+
+class Decoder:
+    """wldpc_decoder handle: ldpc_decoder(rate, z, max_iter, threads) plus batch calls."""
+
+    def __init__(self, rate: int, z: int, max_iter: int = 10, mode: int = MODE_NMS, num_threads: int = 1):
+        self.rate, self.z, self.max_iter, self.mode = rate, z, max_iter, mode
+        self.info = code_info(rate, z)
+        self.n, self.k = self.info.n, self.info.k
+        h = ctypes.c_void_p()
+        _check(_lib().wldpc_decoder_create(rate, z, max_iter, num_threads, mode, ctypes.byref(h)), "decoder")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib().wldpc_decoder_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- reference methods (single frame, host memory) ---
+    def decode(self, rx: np.ndarray):
+        """decode(float*, int8_t*): returns (posterior, decoded, num_errors, iterations)."""
+        post = np.ascontiguousarray(rx, np.float32).copy()
+        dec = np.empty(self.n, np.int8)
+        ne, it = _u(), _i()
+        _check(_lib().wldpc_decoder_decode(self._h, _np_ptr(post), _np_ptr(dec), ctypes.byref(ne),
+                                           ctypes.byref(it)), "decode")
+        return post, dec, ne.value, it.value
+
+    def decode_bits(self, bits: np.ndarray):
+        b = np.ascontiguousarray(bits, np.int8)
+        dec = np.empty(self.n, np.int8)
+        ne = _u()
+        _check(_lib().wldpc_decoder_decode_bits(self._h, _np_ptr(b), _np_ptr(dec), ctypes.byref(ne)), "decode_bits")
+        return dec, ne.value
+
+    def compute_syndrome(self, bits: np.ndarray, exit_early: bool = False) -> int:
+        b = np.ascontiguousarray(bits, np.int8)
+        ne = _u()
+        _check(_lib().wldpc_decoder_compute_syndrome(self._h, _np_ptr(b), int(exit_early), ctypes.byref(ne)),
+               "compute_syndrome")
+        return ne.value
+
+    # --- batch ---
+    def decode_host(self, llr: np.ndarray):
+        """frames x n host batch; returns (posterior, decoded, num_errors, status)."""
+        post = np.ascontiguousarray(llr, np.float32).copy()
+        frames = post.shape[0]
+        dec = np.empty(post.shape, np.int8)
+        ne = np.empty(frames, np.uint32)
+        st = np.empty(frames, np.int32)
+        _check(_lib().wldpc_decode_batch_host(self._h, _np_ptr(post), _np_ptr(dec), _np_ptr(ne), _np_ptr(st),
+                                              frames), "decode_batch_host")
+        return post, dec, ne, st
+
+    def decode_host_into(self, rx, decoded, num_errors=None, status=None):
+        """In-place host batch on caller buffers (numpy or pinned torch CPU tensors)."""
+        ptr = _np_ptr if isinstance(rx, np.ndarray) else _t_ptr
+        frames = rx.shape[0]
+        _check(_lib().wldpc_decode_batch_host(self._h, ptr(rx), ptr(decoded), ptr(num_errors), ptr(status),
+                                              frames), "decode_batch_host")
+
+    def decode_device(self, llr, decoded, posterior=None, status=None, stream=None):
+        """torch CUDA tensors, asynchronous on `stream` (default: torch's current stream)."""
+        frames = llr.shape[0]
+        _check(_lib().wldpc_decode_batch_device(self._h, _t_ptr(llr), _t_ptr(decoded), _t_ptr(posterior),
+                                                _t_ptr(status), frames, _stream_ptr(stream)), "decode_batch_device")
+
+    def synchronize(self):
+        _check(_lib().wldpc_decoder_synchronize(self._h), "synchronize")
+
+
+class Encoder:
+    def __init__(self, rate: int, z: int, num_threads: int = 1):
+        self.rate, self.z = rate, z
+        self.info = code_info(rate, z)
+        self.n, self.k = self.info.n, self.info.k
+        h = ctypes.c_void_p()
+        _check(_lib().wldpc_encoder_create(rate, z, num_threads, ctypes.byref(h)), "encoder")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib().wldpc_encoder_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def encode(self, info: np.ndarray) -> np.ndarray:
+        u = np.ascontiguousarray(info, np.uint8)
+        cw = np.empty(self.n, np.uint8)
+        _check(_lib().wldpc_encoder_encode(self._h, _np_ptr(u), _np_ptr(cw)), "encode")
+        return cw
+
+    def encode_device(self, info, codeword, stream=None):
+        _check(_lib().wldpc_encode_batch_device(self._h, _t_ptr(info), _t_ptr(codeword), info.shape[0],
+                                                _stream_ptr(stream)), "encode_batch_device")
+
+
+def framegen_device(rate, z, seed, first_frame, frames, ebno_lo, ebno_hi=None, info=None, codeword=None,
+                    llr=None, ebno=None, stream=None):
+    """Seeded synthetic frames into torch CUDA tensors (any may be None)."""
+    ebno_hi = ebno_lo if ebno_hi is None else ebno_hi
+    _check(_lib().wldpc_framegen_device(rate, z, seed, first_frame, frames, ebno_lo, ebno_hi, _t_ptr(info),
+                                        _t_ptr(codeword), _t_ptr(llr), _t_ptr(ebno), _stream_ptr(stream)),
+           "framegen")
+
+
+class BERRunner:
+    def __init__(self, rate: int, z: int, num_threads: int = 1, max_iter: int = 10):
+        h = ctypes.c_void_p()
+        _check(_lib().wldpc_ber_runner_create(rate, z, num_threads, max_iter, ctypes.byref(h)), "BER_runner")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib().wldpc_ber_runner_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run_iteration(self, ebno_db: float) -> float:
+        b = ctypes.c_double()
+        _check(_lib().wldpc_ber_runner_run_iteration(self._h, ebno_db, ctypes.byref(b)), "run_iteration")
+        return b.value
+
+    def reset_test(self):
+        _lib().wldpc_ber_runner_reset(self._h)
+
+    def totals(self):
+        b, e = ctypes.c_uint64(), ctypes.c_uint64()
+        _lib().wldpc_ber_runner_totals(self._h, ctypes.byref(b), ctypes.byref(e))
+        return b.value, e.value
+
+    def lengths(self):
+        c, d = _u(), _u()
+        _lib().wldpc_ber_runner_lengths(self._h, ctypes.byref(c), ctypes.byref(d))
+        return c.value, d.value

@@ -1,0 +1,541 @@
+/*
+ * C ABI (include/wimax_ldpc_b200.h) over the sm_100a kernels.
+ *
+ * Handles own their CUDA stream and device scratch; buffers passed in are the
+ * caller's. Single-frame calls keep the reference's synchronous, in-place
+ * semantics (reference lib/ldpc_decoder.cc:122-262): copy in, decode on the
+ * GPU, copy the posterior and hard bits back.
+ */
+#include <cstdint>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <random>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "wimax_ldpc_b200.h"
+#include "codec_kernels.cuh"
+
+using namespace wldpc;
+
+namespace {
+
+int check_device()
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+        cudaGetLastError();
+        return WLDPC_ERR_NO_DEVICE;
+    }
+    return WLDPC_OK;
+}
+
+inline bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+#define CU(call)                                  \
+    do {                                          \
+        if ((call) != cudaSuccess) {              \
+            cudaGetLastError();                   \
+            return WLDPC_ERR_CUDA;                \
+        }                                         \
+    } while (0)
+
+/* grow-only device buffer */
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t want)
+    {
+        if (want <= bytes) return WLDPC_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        if (cudaMalloc(&p, want) != cudaSuccess) {
+            cudaGetLastError();
+            return WLDPC_ERR_CUDA;
+        }
+        bytes = want;
+        return WLDPC_OK;
+    }
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+};
+
+}  // namespace
+
+struct wldpc_decoder {
+    int rate, z, mode;
+    unsigned max_iter;
+    CodeDesc code;
+    cudaStream_t stream = nullptr;
+    cudaStream_t pipe[2] = {nullptr, nullptr};
+    unsigned* err = nullptr;   /* device error word */
+    DevBuf llr, hard, status, bits;
+    DevBuf pllr[2], phard[2], pstatus[2];
+};
+
+struct wldpc_encoder {
+    int rate, z;
+    CodeDesc code;
+    cudaStream_t stream = nullptr;
+    DevBuf info, cw;
+};
+
+struct wldpc_ber_runner {
+    wldpc_encoder* enc = nullptr;
+    wldpc_decoder* dec = nullptr;
+    uint64_t num_bits = 0, num_errors = 0;
+    unsigned codeword_len = 0, dataword_len = 0;
+    float float_rate = 0.f;
+    uint32_t lfsr = 0xdeadbeefu, lfsr_start = 0xdeadbeefu;
+    unsigned lfsr_index = 0, lfsr_reset_len = 1152 * 100;
+    std::mt19937 gen{0};
+    std::normal_distribution<float> dist{0.0f, 1.0f};
+};
+
+extern "C" {
+
+const char* wldpc_strerror(int code)
+{
+    switch (code) {
+    case WLDPC_OK: return "ok";
+    case WLDPC_ERR_ARG: return "invalid argument";
+    case WLDPC_ERR_CODE: return "invalid code rate or z factor";
+    case WLDPC_ERR_CUDA: return "CUDA error";
+    case WLDPC_ERR_NO_DEVICE: return "no CUDA device";
+    case WLDPC_ERR_TIMEOUT: return "device-side wait timed out";
+    case WLDPC_ERR_UNSUPPORTED: return "operation not supported for this code";
+    default: return "unknown error";
+    }
+}
+
+int wldpc_version(void) { return 10000; }
+
+int wldpc_code_info_get(int rate, unsigned z, wldpc_code_info* out)
+{
+    if (!out) return WLDPC_ERR_ARG;
+    if (!valid_rate(rate) || !valid_z((int)z)) return WLDPC_ERR_CODE;
+    const CodeDesc c = make_code_desc(rate, (int)z);
+    out->rate = rate;
+    out->z = (int)z;
+    out->n = c.n;
+    out->m = c.m;
+    out->k = c.k;
+    out->rows = c.m;
+    out->cols = max_degree(rate);
+    out->D = c.D;
+    out->X = c.X;
+    out->layers = c.mb;
+    out->edges = c.nblk * c.z;
+    return WLDPC_OK;
+}
+
+int wldpc_checknode_table(int rate, unsigned z, int16_t* out, size_t capacity)
+{
+    if (!out) return WLDPC_ERR_ARG;
+    if (!valid_rate(rate) || !valid_z((int)z)) return WLDPC_ERR_CODE;
+    const CodeDesc c = make_code_desc(rate, (int)z);
+    const int cols = max_degree(rate);
+    if (capacity < (size_t)c.m * cols) return WLDPC_ERR_ARG;
+    for (int i = 0; i < c.mb; i++)
+        for (int r = 0; r < c.z; r++) {
+            int16_t* row = out + (size_t)(i * c.z + r) * cols;
+            int e = 0;
+            for (int b = c.row_start[i]; b < c.row_start[i + 1]; b++) {
+                int t = r + c.shift[b];
+                t = t >= c.z ? t - c.z : t;
+                row[e++] = (int16_t)(c.col[b] * c.z + t);
+            }
+            for (; e < cols; e++) row[e] = -1;
+        }
+    return WLDPC_OK;
+}
+
+/* ------------------------------------------------------------- decoder */
+
+int wldpc_decoder_create(int rate, unsigned z, unsigned max_iter, unsigned num_threads, int mode,
+                         wldpc_decoder** out)
+{
+    (void)num_threads;
+    if (!out) return WLDPC_ERR_ARG;
+    *out = nullptr;
+    if (!valid_rate(rate) || !valid_z((int)z)) return WLDPC_ERR_CODE;
+    if (mode < WLDPC_MODE_NMS || mode > WLDPC_MODE_MS || max_iter > 0xffff) return WLDPC_ERR_ARG;
+    int rc = check_device();
+    if (rc) return rc;
+    wldpc_decoder* d = new (std::nothrow) wldpc_decoder();
+    if (!d) return WLDPC_ERR_ARG;
+    d->rate = rate;
+    d->z = (int)z;
+    d->mode = mode;
+    d->max_iter = max_iter;
+    d->code = make_code_desc(rate, (int)z);
+    if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&d->err, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(d->err, 0, sizeof(unsigned)) != cudaSuccess) {
+        cudaGetLastError();
+        wldpc_decoder_destroy(d);
+        return WLDPC_ERR_CUDA;
+    }
+    *out = d;
+    return WLDPC_OK;
+}
+
+int wldpc_decoder_destroy(wldpc_decoder* d)
+{
+    if (!d) return WLDPC_ERR_ARG;
+    if (d->stream) cudaStreamSynchronize(d->stream);
+    for (auto& s : d->pipe)
+        if (s) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+        }
+    if (d->stream) cudaStreamDestroy(d->stream);
+    if (d->err) cudaFree(d->err);
+    delete d;
+    return WLDPC_OK;
+}
+
+static int decode_launch(wldpc_decoder* d, const float* llr, int8_t* hard, float* post, int32_t* status,
+                         size_t frames, cudaStream_t st)
+{
+    DecodeArgs a;
+    a.llr = llr;
+    a.hard = hard;
+    a.post = post;
+    a.status = status;
+    a.err = d->err;
+    a.frames = (long long)frames;
+    a.max_iter = (int)d->max_iter;
+    return launch_tdmp(d->rate, d->z, d->mode, a, st) == cudaSuccess ? WLDPC_OK : WLDPC_ERR_CUDA;
+}
+
+static int read_err(wldpc_decoder* d)
+{
+    unsigned e = 0;
+    CU(cudaMemcpy(&e, d->err, sizeof(e), cudaMemcpyDeviceToHost));
+    if (e) {
+        CU(cudaMemset(d->err, 0, sizeof(unsigned)));
+        return WLDPC_ERR_TIMEOUT;
+    }
+    return WLDPC_OK;
+}
+
+int wldpc_decode_batch_device(wldpc_decoder* d, const float* llr, int8_t* decoded, float* posterior,
+                              int32_t* status, size_t frames, void* stream)
+{
+    if (!d || (frames && (!llr || !decoded))) return WLDPC_ERR_ARG;
+    if (!aligned(llr, 16) || !aligned(decoded, 4) || !aligned(posterior, 16) || !aligned(status, 4))
+        return WLDPC_ERR_ARG;
+    if (frames == 0) return WLDPC_OK;
+    return decode_launch(d, llr, decoded, posterior, status, frames, (cudaStream_t)stream);
+}
+
+int wldpc_decoder_synchronize(wldpc_decoder* d)
+{
+    if (!d) return WLDPC_ERR_ARG;
+    CU(cudaDeviceSynchronize());
+    return read_err(d);
+}
+
+static int decode_frames_host(wldpc_decoder* d, float* rx, int8_t* decoded, int32_t* status_host,
+                              size_t frames)
+{
+    const size_t n = (size_t)d->code.n;
+    int rc;
+    if ((rc = d->llr.reserve(frames * n * 4)) || (rc = d->hard.reserve(frames * n)) ||
+        (rc = d->status.reserve(frames * 4)))
+        return rc;
+    CU(cudaMemcpyAsync(d->llr.p, rx, frames * n * 4, cudaMemcpyHostToDevice, d->stream));
+    if ((rc = decode_launch(d, (const float*)d->llr.p, (int8_t*)d->hard.p, (float*)d->llr.p,
+                            (int32_t*)d->status.p, frames, d->stream)))
+        return rc;
+    CU(cudaMemcpyAsync(rx, d->llr.p, frames * n * 4, cudaMemcpyDeviceToHost, d->stream));
+    CU(cudaMemcpyAsync(decoded, d->hard.p, frames * n, cudaMemcpyDeviceToHost, d->stream));
+    CU(cudaMemcpyAsync(status_host, d->status.p, frames * 4, cudaMemcpyDeviceToHost, d->stream));
+    CU(cudaStreamSynchronize(d->stream));
+    return read_err(d);
+}
+
+static unsigned ref_return(const wldpc_decoder* d, int32_t status)
+{
+    return d->max_iter == 0 ? 0u : (unsigned)((status >> 16) & 1);
+}
+
+int wldpc_decoder_decode(wldpc_decoder* d, float* rx_codeword, int8_t* decoded, unsigned* num_errors,
+                         int* iterations)
+{
+    if (!d || !rx_codeword || !decoded) return WLDPC_ERR_ARG;
+    int32_t st = 0;
+    int rc = decode_frames_host(d, rx_codeword, decoded, &st, 1);
+    if (rc) return rc;
+    if (num_errors) *num_errors = ref_return(d, st);
+    if (iterations) *iterations = st & 0xffff;
+    return WLDPC_OK;
+}
+
+int wldpc_decoder_decode_bits(wldpc_decoder* d, const int8_t* rx_codeword, int8_t* decoded,
+                              unsigned* num_errors)
+{
+    if (!d || !rx_codeword || !decoded) return WLDPC_ERR_ARG;
+    const size_t n = (size_t)d->code.n;
+    int rc;
+    if ((rc = d->llr.reserve(n * 4)) || (rc = d->hard.reserve(n)) || (rc = d->status.reserve(4)) ||
+        (rc = d->bits.reserve(n)))
+        return rc;
+    CU(cudaMemcpyAsync(d->bits.p, rx_codeword, n, cudaMemcpyHostToDevice, d->stream));
+    CU(launch_bits_to_llr((const int8_t*)d->bits.p, (float*)d->llr.p, (long long)n, d->stream));
+    if ((rc = decode_launch(d, (const float*)d->llr.p, (int8_t*)d->hard.p, nullptr, (int32_t*)d->status.p, 1,
+                            d->stream)))
+        return rc;
+    int32_t st = 0;
+    CU(cudaMemcpyAsync(decoded, d->hard.p, n, cudaMemcpyDeviceToHost, d->stream));
+    CU(cudaMemcpyAsync(&st, d->status.p, 4, cudaMemcpyDeviceToHost, d->stream));
+    CU(cudaStreamSynchronize(d->stream));
+    if ((rc = read_err(d))) return rc;
+    if (num_errors) *num_errors = ref_return(d, st);
+    return WLDPC_OK;
+}
+
+int wldpc_decoder_compute_syndrome(wldpc_decoder* d, const int8_t* rx_codeword, int exit_early,
+                                   unsigned* num_errors)
+{
+    if (!d || !rx_codeword || !num_errors) return WLDPC_ERR_ARG;
+    const size_t n = (size_t)d->code.n;
+    int rc;
+    if ((rc = d->bits.reserve(n)) || (rc = d->status.reserve(4))) return rc;
+    CU(cudaMemcpyAsync(d->bits.p, rx_codeword, n, cudaMemcpyHostToDevice, d->stream));
+    CU(launch_syndrome(d->code, (const int8_t*)d->bits.p, (uint32_t*)d->status.p, 1, exit_early, d->stream));
+    uint32_t v = 0;
+    CU(cudaMemcpyAsync(&v, d->status.p, 4, cudaMemcpyDeviceToHost, d->stream));
+    CU(cudaStreamSynchronize(d->stream));
+    *num_errors = v;
+    return WLDPC_OK;
+}
+
+/* Host batch: chunks alternate between two streams so that the copy-in of
+ * one chunk, the kernel of another and the copy-out of a third overlap. */
+int wldpc_decode_batch_host(wldpc_decoder* d, float* rx, int8_t* decoded, uint32_t* num_errors,
+                            int32_t* status, size_t frames)
+{
+    if (!d || (frames && (!rx || !decoded))) return WLDPC_ERR_ARG;
+    if (frames == 0) return WLDPC_OK;
+    const size_t n = (size_t)d->code.n;
+    const size_t chunk = frames < 32768 ? frames : 32768;
+    int rc;
+    for (int s = 0; s < 2; s++) {
+        if (!d->pipe[s]) CU(cudaStreamCreateWithFlags(&d->pipe[s], cudaStreamNonBlocking));
+        if ((rc = d->pllr[s].reserve(chunk * n * 4)) || (rc = d->phard[s].reserve(chunk * n)) ||
+            (rc = d->pstatus[s].reserve(chunk * 4)))
+            return rc;
+    }
+    std::vector<int32_t> st_local;
+    int32_t* st_host = status;
+    if (!st_host && num_errors) {
+        st_local.resize(frames);
+        st_host = st_local.data();
+    }
+    size_t idx = 0;
+    for (size_t f0 = 0; f0 < frames; f0 += chunk, idx++) {
+        const int s = (int)(idx & 1);
+        const size_t nf = frames - f0 < chunk ? frames - f0 : chunk;
+        cudaStream_t st = d->pipe[s];
+        CU(cudaMemcpyAsync(d->pllr[s].p, rx + f0 * n, nf * n * 4, cudaMemcpyHostToDevice, st));
+        if ((rc = decode_launch(d, (const float*)d->pllr[s].p, (int8_t*)d->phard[s].p, (float*)d->pllr[s].p,
+                                (int32_t*)d->pstatus[s].p, nf, st)))
+            return rc;
+        CU(cudaMemcpyAsync(rx + f0 * n, d->pllr[s].p, nf * n * 4, cudaMemcpyDeviceToHost, st));
+        CU(cudaMemcpyAsync(decoded + f0 * n, d->phard[s].p, nf * n, cudaMemcpyDeviceToHost, st));
+        if (st_host) CU(cudaMemcpyAsync(st_host + f0, d->pstatus[s].p, nf * 4, cudaMemcpyDeviceToHost, st));
+    }
+    CU(cudaStreamSynchronize(d->pipe[0]));
+    CU(cudaStreamSynchronize(d->pipe[1]));
+    if ((rc = read_err(d))) return rc;
+    if (num_errors)
+        for (size_t f = 0; f < frames; f++) num_errors[f] = ref_return(d, st_host[f]);
+    return WLDPC_OK;
+}
+
+/* ------------------------------------------------------------- encoder */
+
+int wldpc_encoder_create(int rate, unsigned z, unsigned num_threads, wldpc_encoder** out)
+{
+    (void)num_threads;
+    if (!out) return WLDPC_ERR_ARG;
+    *out = nullptr;
+    if (!valid_rate(rate) || !valid_z((int)z)) return WLDPC_ERR_CODE;
+    int rc = check_device();
+    if (rc) return rc;
+    wldpc_encoder* e = new (std::nothrow) wldpc_encoder();
+    if (!e) return WLDPC_ERR_ARG;
+    e->rate = rate;
+    e->z = (int)z;
+    e->code = make_code_desc(rate, (int)z);
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete e;
+        return WLDPC_ERR_CUDA;
+    }
+    *out = e;
+    return WLDPC_OK;
+}
+
+int wldpc_encoder_destroy(wldpc_encoder* e)
+{
+    if (!e) return WLDPC_ERR_ARG;
+    if (e->stream) {
+        cudaStreamSynchronize(e->stream);
+        cudaStreamDestroy(e->stream);
+    }
+    delete e;
+    return WLDPC_OK;
+}
+
+int wldpc_encode_batch_device(wldpc_encoder* e, const uint8_t* info, uint8_t* codeword, size_t frames,
+                              void* stream)
+{
+    if (!e || (frames && (!info || !codeword))) return WLDPC_ERR_ARG;
+    if (!aligned(info, 4) || !aligned(codeword, 4)) return WLDPC_ERR_ARG;
+    CU(launch_encode_bytes(e->code, info, codeword, (long long)frames, (cudaStream_t)stream));
+    return WLDPC_OK;
+}
+
+int wldpc_encoder_encode(wldpc_encoder* e, const uint8_t* infoword, uint8_t* codeword)
+{
+    if (!e || !infoword || !codeword) return WLDPC_ERR_ARG;
+    int rc;
+    if ((rc = e->info.reserve((size_t)e->code.k)) || (rc = e->cw.reserve((size_t)e->code.n))) return rc;
+    CU(cudaMemcpyAsync(e->info.p, infoword, (size_t)e->code.k, cudaMemcpyHostToDevice, e->stream));
+    CU(launch_encode_bytes(e->code, (const uint8_t*)e->info.p, (uint8_t*)e->cw.p, 1, e->stream));
+    CU(cudaMemcpyAsync(codeword, e->cw.p, (size_t)e->code.n, cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaStreamSynchronize(e->stream));
+    return WLDPC_OK;
+}
+
+/* ----------------------------------------------------------- framegen */
+
+int wldpc_framegen_device(int rate, unsigned z, uint64_t seed, uint64_t first_frame, size_t frames,
+                          float ebno_lo_db, float ebno_hi_db, uint8_t* info, uint8_t* codeword, float* llr,
+                          float* ebno_db, void* stream)
+{
+    if (!valid_rate(rate) || !valid_z((int)z)) return WLDPC_ERR_CODE;
+    if (rate == THREEQUARTERSB) return WLDPC_ERR_UNSUPPORTED;
+    if (!aligned(info, 4) || !aligned(codeword, 4) || !aligned(llr, 16) || !aligned(ebno_db, 4))
+        return WLDPC_ERR_ARG;
+    int rc = check_device();
+    if (rc) return rc;
+    FramegenArgs a;
+    a.seed = seed;
+    a.first_frame = first_frame;
+    a.frames = (long long)frames;
+    a.ebno_lo = ebno_lo_db;
+    a.ebno_hi = ebno_hi_db;
+    a.info = info;
+    a.cw = codeword;
+    a.llr = llr;
+    a.ebno_out = ebno_db;
+    CU(launch_framegen(make_code_desc(rate, (int)z), a, (cudaStream_t)stream));
+    return WLDPC_OK;
+}
+
+/* ---------------------------------------------------------- BER runner */
+
+int wldpc_ber_runner_create(int rate, unsigned z, unsigned num_threads, unsigned max_iter,
+                            wldpc_ber_runner** out)
+{
+    if (!out) return WLDPC_ERR_ARG;
+    *out = nullptr;
+    if (!valid_rate(rate) || !valid_z((int)z)) return WLDPC_ERR_CODE;
+    if (rate == THREEQUARTERSB) return WLDPC_ERR_UNSUPPORTED;   /* reference lib/BER_runner.cc:66-71 */
+    wldpc_ber_runner* b = new (std::nothrow) wldpc_ber_runner();
+    if (!b) return WLDPC_ERR_ARG;
+    int rc = wldpc_encoder_create(rate, z, num_threads, &b->enc);
+    if (!rc) rc = wldpc_decoder_create(rate, z, max_iter, num_threads, WLDPC_MODE_NMS, &b->dec);
+    if (rc) {
+        wldpc_ber_runner_destroy(b);
+        return rc;
+    }
+    /* lengths and rate as the reference computes them (reference :30,43-77) */
+    b->codeword_len = (unsigned)((z / 96.0) * 2304);
+    static const float kRate[6] = {0.5f, (float)(2.0 / 3.0), (float)(2.0 / 3.0), (float)(3.0 / 4.0), 0.f,
+                                   (float)(5.0 / 6.0)};
+    static const unsigned kNum[6] = {1, 2, 2, 3, 0, 5}, kDen[6] = {2, 3, 3, 4, 1, 6};
+    b->dataword_len = (b->codeword_len * kNum[rate]) / kDen[rate];
+    b->float_rate = kRate[rate];
+    *out = b;
+    return WLDPC_OK;
+}
+
+int wldpc_ber_runner_destroy(wldpc_ber_runner* b)
+{
+    if (!b) return WLDPC_ERR_ARG;
+    if (b->enc) wldpc_encoder_destroy(b->enc);
+    if (b->dec) wldpc_decoder_destroy(b->dec);
+    delete b;
+    return WLDPC_OK;
+}
+
+int wldpc_ber_runner_run_iteration(wldpc_ber_runner* b, double ebno_db, double* ber)
+{
+    if (!b) return WLDPC_ERR_ARG;
+    const unsigned n = b->codeword_len, k = b->dataword_len;
+    std::vector<uint8_t> data(k), cw(n);
+    std::vector<float> buf(n);
+    std::vector<int8_t> dec(n);
+    const double ebno_lin = pow(10.0, ebno_db / 10.0);
+    const float amp = (float)((1.0 / std::sqrt(ebno_lin)) * std::sqrt(1.0 / (b->float_rate * 1)));
+    /* info bits: LFSR x^31 + x^28 + 1, restarted every reset_len bits (reference :124-146) */
+    for (unsigned i = 0; i < k; i++) {
+        const uint32_t bit = ((b->lfsr >> 0) ^ (b->lfsr >> 3)) & 1u;
+        b->lfsr = (b->lfsr >> 1) | (bit << 30);
+        if (++b->lfsr_index == b->lfsr_reset_len) {
+            b->lfsr = b->lfsr_start;
+            b->lfsr_index = 0;
+        }
+        data[i] = (uint8_t)bit;
+    }
+    int rc = wldpc_encoder_encode(b->enc, data.data(), cw.data());
+    if (rc) return rc;
+    /* BPSK and the reference's noise stream, in its order and types (reference :181-191) */
+    for (unsigned j = 0; j < n; j++) buf[j] = (float)(cw[j] * 2 - 1);
+    for (unsigned j = 0; j < n; j++) buf[j] = buf[j] + std::sqrt(0.5) * amp * b->dist(b->gen);
+    unsigned ne = 0;
+    rc = wldpc_decoder_decode(b->dec, buf.data(), dec.data(), &ne, nullptr);
+    if (rc) return rc;
+    b->num_bits += k;
+    unsigned errors = 0;   /* counted over all n codeword bits (reference :148-160) */
+    for (unsigned j = 0; j < n; j++) errors += cw[j] != (uint8_t)dec[j];
+    b->num_errors += errors;
+    if (ber) *ber = (double)b->num_errors / (double)b->num_bits;
+    return WLDPC_OK;
+}
+
+int wldpc_ber_runner_reset(wldpc_ber_runner* b)
+{
+    if (!b) return WLDPC_ERR_ARG;
+    b->num_bits = 0;
+    b->num_errors = 0;
+    return WLDPC_OK;
+}
+
+int wldpc_ber_runner_totals(wldpc_ber_runner* b, uint64_t* num_bits, uint64_t* num_errors)
+{
+    if (!b) return WLDPC_ERR_ARG;
+    if (num_bits) *num_bits = b->num_bits;
+    if (num_errors) *num_errors = b->num_errors;
+    return WLDPC_OK;
+}
+
+int wldpc_ber_runner_lengths(wldpc_ber_runner* b, unsigned* codeword_len, unsigned* dataword_len)
+{
+    if (!b) return WLDPC_ERR_ARG;
+    if (codeword_len) *codeword_len = b->codeword_len;
+    if (dataword_len) *dataword_len = b->dataword_len;
+    return WLDPC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,230 @@
+/*
+ * Encoder, frame generation, syndrome and input-adapter kernels.
+ *
+ *  encode_bytes_kernel  - ldpc_encoder::encode_data over a batch
+ *                         (reference lib/ldpc_encoder.cc:50-105), one warp per frame
+ *  framegen_kernel      - seeded synthetic frames: Philox info bits, the same
+ *                         encoder on packed words, BPSK bit*2-1 (reference
+ *                         lib/BER_runner.cc:183), AWGN, LLR = 2y/sigma^2
+ *  syndrome_kernel      - compute_syndrome (reference lib/ldpc_decoder.cc:67-104)
+ *  bits_to_llr_kernel   - the int8 input adapter bit*2.0-1.0 (reference
+ *                         lib/ldpc_decoder.cc:108-118)
+ */
+#include <cstdint>
+#include "codec_kernels.cuh"
+
+namespace wldpc {
+
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int round = 0; round < 10; round++) {
+        const uint32_t lo0 = 0xD2511F53u * c[0], hi0 = __umulhi(0xD2511F53u, c[0]);
+        const uint32_t lo1 = 0xCD9E8D57u * c[2], hi1 = __umulhi(0xCD9E8D57u, c[2]);
+        const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+/* Philox block: counter (word, frame lo, frame hi, stream), key = seed */
+__device__ __forceinline__ void philox_at(uint64_t seed, uint64_t frame, uint32_t word, uint32_t stream,
+                                          uint32_t o[4])
+{
+    o[0] = word; o[1] = (uint32_t)frame; o[2] = (uint32_t)(frame >> 32); o[3] = stream;
+    philox4x32_10(o, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+__device__ __forceinline__ float unif24(uint32_t x) { return ((float)(x >> 8) + 0.5f) * (1.0f / 16777216.0f); }
+
+constexpr int kEncWarps = 8;
+
+__global__ void __launch_bounds__(32 * kEncWarps)
+encode_bytes_kernel(CodeDesc c, const uint8_t* __restrict__ info, uint8_t* __restrict__ cw, long long frames)
+{
+    __shared__ EncScratch scratch[kEncWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long f = (long long)blockIdx.x * kEncWarps + warp;
+    if (f >= frames) return;
+    EncScratch& s = scratch[warp];
+    const uint8_t* u = info + f * c.k;
+    uint8_t* x = cw + f * c.n;
+    /* pack: any non-zero byte is a 1 (reference :43) */
+    const int kw = (c.k + 31) / 32;
+    for (int q = 0; q < kw; q++) {
+        const int j = q * 32 + lane;
+        const uint32_t w = __ballot_sync(0xffffffffu, j < c.k && u[j] != 0);
+        if (lane == 0) s.U[q] = w;
+    }
+    if (lane < 4) s.U[kw + lane] = 0;
+    __syncwarp();
+    warp_encode_parity(c, s, lane);
+    /* systematic copy of the raw bytes (k is a multiple of 4) */
+    const uint32_t* u4 = reinterpret_cast<const uint32_t*>(u);
+    uint32_t* x4 = reinterpret_cast<uint32_t*>(x);
+    for (int j = lane; j < c.k / 4; j += 32) x4[j] = u4[j];
+    /* parity bytes */
+    for (int b = 0; b < c.mb; b++)
+        for (int r = lane * 4; r < c.z; r += 128)
+            x4[(c.k + b * c.z + r) / 4] = parity_bytes4(s, c.nw, b, r);
+}
+
+__global__ void __launch_bounds__(32 * kEncWarps)
+framegen_kernel(CodeDesc c, FramegenArgs a)
+{
+    __shared__ EncScratch scratch[kEncWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long f = (long long)blockIdx.x * kEncWarps + warp;
+    if (f >= a.frames) return;
+    EncScratch& s = scratch[warp];
+    const uint64_t g = a.first_frame + (uint64_t)f;
+    /* info bits: Philox stream 0, 128 bits per block */
+    const int kblk = (c.k + 127) / 128;
+    for (int q = lane; q < kblk; q += 32) {
+        uint32_t o[4];
+        philox_at(a.seed, g, (uint32_t)q, 0u, o);
+#pragma unroll
+        for (int t = 0; t < 4; t++) s.U[4 * q + t] = o[t];
+    }
+    __syncwarp();
+    /* clear the bits past k so that packed views stay canonical */
+    if (lane == 0) {
+        const int kw = (c.k + 31) / 32;
+        if (c.k & 31) s.U[kw - 1] &= (1u << (c.k & 31)) - 1u;
+        for (int t = kw; t < kw + 4; t++) s.U[t] = 0;
+    }
+    __syncwarp();
+    warp_encode_parity(c, s, lane);
+
+    /* per-frame Eb/N0 and noise scale, in float */
+    uint32_t eo[4];
+    philox_at(a.seed, g, 0u, 2u, eo);
+    const float ebno = __fadd_rn(a.ebno_lo, __fmul_rn(__fsub_rn(a.ebno_hi, a.ebno_lo), unif24(eo[0])));
+    const float rate = (float)c.k / (float)c.n;
+    const float ebno_lin = exp10f(ebno * 0.1f);
+    const float sigma2 = 1.0f / (2.0f * rate * ebno_lin);
+    const float sigma = sqrtf(sigma2);
+    const float scale = 2.0f / sigma2;
+    if (a.ebno_out && lane == 0) a.ebno_out[f] = ebno;
+
+    if (a.info) {
+        uint32_t* i4 = reinterpret_cast<uint32_t*>(a.info + f * c.k);
+        for (int j = lane * 4; j < c.k; j += 128) {
+            const uint32_t w = s.U[j >> 5] >> (j & 31);
+            i4[j >> 2] = (w & 1u) | ((w & 2u) << 7) | ((w & 4u) << 14) | ((w & 8u) << 21);
+        }
+    }
+    if (a.cw) {
+        uint32_t* x4 = reinterpret_cast<uint32_t*>(a.cw + f * c.n);
+        for (int j = lane * 4; j < c.k; j += 128) {
+            const uint32_t w = s.U[j >> 5] >> (j & 31);
+            x4[j >> 2] = (w & 1u) | ((w & 2u) << 7) | ((w & 4u) << 14) | ((w & 8u) << 21);
+        }
+        for (int b = 0; b < c.mb; b++)
+            for (int r = lane * 4; r < c.z; r += 128)
+                x4[(c.k + b * c.z + r) >> 2] = parity_bytes4(s, c.nw, b, r);
+    }
+    if (a.llr) {
+        float4* l4 = reinterpret_cast<float4*>(a.llr + f * c.n);
+        for (int j = lane * 4; j < c.n; j += 128) {
+            uint32_t bits;
+            if (j < c.k) {
+                bits = s.U[j >> 5] >> (j & 31);
+            } else {
+                const int p = j - c.k, b = p / c.z, r = p - b * c.z;
+                bits = s.out[b * c.nw + (r >> 5)] >> (r & 31);
+            }
+            uint32_t o[4];
+            philox_at(a.seed, g, (uint32_t)(j >> 2), 1u, o);
+            float nrm[4];
+#pragma unroll
+            for (int p = 0; p < 2; p++) {
+                const float u1 = unif24(o[2 * p]), u2 = unif24(o[2 * p + 1]);
+                const float rad = sqrtf(-2.0f * logf(u1));
+                float sn, cs;
+                sincospif(2.0f * u2, &sn, &cs);
+                nrm[2 * p] = rad * cs;
+                nrm[2 * p + 1] = rad * sn;
+            }
+            float4 v;
+            v.x = scale * ((bits & 1u ? 1.0f : -1.0f) + sigma * nrm[0]);
+            v.y = scale * ((bits & 2u ? 1.0f : -1.0f) + sigma * nrm[1]);
+            v.z = scale * ((bits & 4u ? 1.0f : -1.0f) + sigma * nrm[2]);
+            v.w = scale * ((bits & 8u ? 1.0f : -1.0f) + sigma * nrm[3]);
+            l4[j >> 2] = v;
+        }
+    }
+}
+
+/* One thread per expanded check row; rows of a frame are contiguous in
+ * threadIdx.x. out[f] = number of failing rows, or 0/1 with early_exit. */
+__global__ void syndrome_kernel(CodeDesc c, const int8_t* __restrict__ bits, uint32_t* __restrict__ out,
+                                long long frames, int early_exit)
+{
+    const long long f = blockIdx.x;
+    if (f >= frames) return;
+    const int8_t* x = bits + f * c.n;
+    __shared__ uint32_t count;
+    if (threadIdx.x == 0) count = 0;
+    __syncthreads();
+    uint32_t local = 0;
+    for (int row = threadIdx.x; row < c.m; row += blockDim.x) {
+        const int i = row / c.z, r = row - i * c.z;
+        int8_t acc = 0;
+        for (int b = c.row_start[i]; b < c.row_start[i + 1]; b++) {
+            int t = r + c.shift[b];
+            t = t >= c.z ? t - c.z : t;
+            acc ^= x[c.col[b] * c.z + t];
+        }
+        local += acc != 0;
+    }
+    if (local) atomicAdd(&count, local);
+    __syncthreads();
+    if (threadIdx.x == 0) out[f] = early_exit ? (count != 0) : count;
+}
+
+__global__ void bits_to_llr_kernel(const int8_t* __restrict__ bits, float* __restrict__ llr, long long count)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        llr[i] = (float)__dadd_rn(__dmul_rn((double)bits[i], 2.0), -1.0);
+}
+
+/* ---------------------------------------------------------------- launchers */
+
+cudaError_t launch_encode_bytes(const CodeDesc& c, const uint8_t* info, uint8_t* cw, long long frames,
+                                cudaStream_t st)
+{
+    if (frames <= 0) return cudaSuccess;
+    const long long blocks = (frames + kEncWarps - 1) / kEncWarps;
+    encode_bytes_kernel<<<(unsigned)blocks, 32 * kEncWarps, 0, st>>>(c, info, cw, frames);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_framegen(const CodeDesc& c, const FramegenArgs& a, cudaStream_t st)
+{
+    if (a.frames <= 0) return cudaSuccess;
+    const long long blocks = (a.frames + kEncWarps - 1) / kEncWarps;
+    framegen_kernel<<<(unsigned)blocks, 32 * kEncWarps, 0, st>>>(c, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_syndrome(const CodeDesc& c, const int8_t* bits, uint32_t* out, long long frames,
+                            int early_exit, cudaStream_t st)
+{
+    if (frames <= 0) return cudaSuccess;
+    syndrome_kernel<<<(unsigned)frames, 256, 0, st>>>(c, bits, out, frames, early_exit);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bits_to_llr(const int8_t* bits, float* llr, long long count, cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    long long blocks = (count + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    bits_to_llr_kernel<<<(unsigned)blocks, 256, 0, st>>>(bits, llr, count);
+    return cudaGetLastError();
+}
+
+}  // namespace wldpc

@@ -1,0 +1,47 @@
+/*
+ * Launchers for the encoder / frame generation / syndrome / input-adapter
+ * kernels (codec_kernels.cu) and the TDMP decoders (tdmp_dispatch.cu).
+ */
+#ifndef WLDPC_CODEC_KERNELS_CUH
+#define WLDPC_CODEC_KERNELS_CUH
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "encode.cuh"
+#include "nms_decode.cuh"
+
+namespace wldpc {
+
+struct FramegenArgs {
+    uint64_t seed;
+    uint64_t first_frame;   /* global index of frame 0 of this batch */
+    long long frames;
+    float ebno_lo, ebno_hi; /* Eb/N0 (dB) drawn uniformly per frame */
+    uint8_t* info;          /* frames x k bytes 0/1, or null */
+    uint8_t* cw;            /* frames x n bytes 0/1, or null */
+    float* llr;             /* frames x n, or null (16-byte aligned) */
+    float* ebno_out;        /* frames, or null */
+};
+
+cudaError_t launch_encode_bytes(const CodeDesc& c, const uint8_t* info, uint8_t* cw, long long frames,
+                                cudaStream_t st);
+cudaError_t launch_framegen(const CodeDesc& c, const FramegenArgs& a, cudaStream_t st);
+cudaError_t launch_syndrome(const CodeDesc& c, const int8_t* bits, uint32_t* out, long long frames,
+                            int early_exit, cudaStream_t st);
+cudaError_t launch_bits_to_llr(const int8_t* bits, float* llr, long long count, cudaStream_t st);
+
+/* TDMP decoder specialised on (rate, z, mode) */
+struct TdmpLaunch {
+    void (*kernel)(const DecodeArgs);
+    int threads;        /* per CTA (run-time z: z) */
+    int frames_per_cta;
+    int smem;           /* dynamic shared memory bytes (run-time z: 96 z) */
+    bool runtime_z;     /* z, shifts and columns are passed in DecodeArgs */
+};
+/* entry for (rate, z, mode) or null if not built */
+const TdmpLaunch* tdmp_entry(int rate, int z, int mode);
+cudaError_t launch_tdmp(int rate, int z, int mode, const DecodeArgs& a, cudaStream_t st);
+
+}  // namespace wldpc
+
+#endif

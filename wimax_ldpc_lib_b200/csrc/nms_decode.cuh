@@ -1,0 +1,286 @@
+/*
+ * Plain layered (TDMP) min-sum decoder for sm_100a, bit-exact with the
+ * reference ldpc_decoder::decode(float*, int8_t*) (reference
+ * lib/ldpc_decoder.cc:122-262), in its three compile-time flavours
+ * (reference lib/ldpc_decoder.cc:17-21,215-238):
+ *   kNms: message = s * float((double)min * 0.815), posterior added in fp64
+ *   kOms: message = s * float(max((double)min - 0.10, 0)), posterior in fp64
+ *   kMs : message = s * min, posterior added in fp32
+ *
+ * Mapping. One CTA decodes G frames, G = 32/gcd(z, 32), so that G*z threads
+ * fill whole warps (z = 96: one frame of 96 threads). Thread (g, r) owns
+ * expanded row r of every layer of frame g. A layer is one base row; its z rows
+ * touch disjoint variables (every block is a z x z circulant), so processing
+ * them concurrently is identical to the reference's sequential row order.
+ * Layers run in table order with a CTA barrier between them, as the reference.
+ *
+ * Data. The frame's LLRs are staged global -> shared with one TMA bulk copy
+ * and updated in place as the posterior (24z floats). Check-to-variable
+ * messages live in registers in compressed form per row: the two rounded
+ * message magnitudes float(D1), float(D2), the argmin edge and one sign bit per
+ * edge. Circulant shifts are compile-time constants: the address of edge e of
+ * row r is col*z + (r + shift) mod z.
+ *
+ * Arithmetic that must round exactly as the reference (x86, no FMA):
+ *   L = post - msg                      float subtract
+ *   D = (double)min * 0.815             __dmul_rn (no contraction)
+ *   msg' = (float)(+-D)                 __double2float_rn
+ *   post' = (float)((double)L +- D)     __dadd_rn then __double2float_rn
+ * The sign test is x < 0 (-0.0 is non-negative), which is how the reference's
+ * -ffast-math build evaluates std::signbit (reference lib/CMakeLists.txt:6);
+ * a canonicalising +0.0f add turns -0.0 into +0.0 before its sign bit is read.
+ * min1/min2 track the two smallest |L| starting from 10000.0f (reference
+ * lib/ldpc_decoder.cc:150,198); an edge whose |L| equals min1 receives min2,
+ * which equals the reference's per-edge recomputation, ties included.
+ *
+ * Stopping rule (reference lib/ldpc_decoder.cc:127-139,241-251): slice
+ * (x >= 0) and check every row after staging and after every iteration; a
+ * frame stops at the first zero syndrome. Outputs: hard bits (int8 0/1),
+ * optionally the posterior, and status = iterations | synfail << 16.
+ */
+#ifndef WLDPC_NMS_DECODE_CUH
+#define WLDPC_NMS_DECODE_CUH
+
+#include <cstdint>
+#include "codes.h"
+#include "device_util.cuh"
+
+namespace wldpc {
+
+enum DecodeMode : int { kNms = 0, kOms = 1, kMs = 2 };
+
+struct DecodeArgs {
+    const float* llr;       /* frames x n, 16-byte aligned */
+    int8_t* hard;           /* frames x n, 4-byte aligned */
+    float* post;            /* frames x n or null, 16-byte aligned (may alias llr) */
+    int32_t* status;        /* frames or null */
+    unsigned* err;          /* error word (kErr*) */
+    long long frames;
+    int max_iter;
+    /* used only by the kernels whose z is a run-time value (ZT == 0): */
+    int z;
+    unsigned short shift[96];   /* per non-zero block, row-major over base rows */
+    unsigned short colz[96];    /* block column * z */
+};
+
+/* Shape of a TDMP launch. ZT > 0: z is a compile-time constant and a CTA
+ * holds G = 32/gcd(z, 32) frames; ZT == 0: z comes from DecodeArgs and a CTA
+ * holds one frame of z threads. */
+template <int R, int ZT>
+struct TdmpShape {
+    static constexpr int MB = kMb[R];
+    static constexpr int G = ZT > 0 ? 32 / gcd_c(ZT, 32) : 1;
+    static constexpr int THREADS = ZT > 0 ? G * ZT : kZMax;
+    static constexpr int SMEM = G * kNB * (ZT > 0 ? ZT : kZMax) * 4;
+};
+
+/* index of the e-th block of base row i in row-major block order */
+constexpr int block_index(int rate, int i, int e)
+{
+    int b = 0;
+    for (int q = 0; q < i; q++) b += layer_degree(rate, q);
+    return b + e;
+}
+
+/* variable index of edge E of layer I for row r */
+template <int R, int ZT, int I, int E>
+__device__ __forceinline__ int edge_var(int r, const DecodeArgs& a)
+{
+    if constexpr (ZT > 0) {
+        constexpr int col = layer_col(R, I, E);
+        constexpr int s = layer_shift(R, ZT, I, E);
+        int t = r + s;
+        t = (t >= ZT) ? t - ZT : t;
+        return col * ZT + t;
+    } else {
+        constexpr int b = block_index(R, I, E);
+        int t = r + (int)a.shift[b];
+        t = (t >= a.z) ? t - a.z : t;
+        return (int)a.colz[b] + t;
+    }
+}
+
+__device__ __forceinline__ float canon(float x) { return __fadd_rn(x, 0.0f); }
+
+template <int R, int ZT, int MODE>
+__global__ void __launch_bounds__(TdmpShape<R, ZT>::THREADS)
+tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
+{
+    using S = TdmpShape<R, ZT>;
+    constexpr int MB = S::MB, G = S::G;
+    const int Z = ZT > 0 ? ZT : a.z;
+    const int N = kNB * Z;
+    const int nthreads = G * Z;
+    extern __shared__ __align__(128) float smem_post[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ unsigned s_fail[2];
+
+    const int tid = threadIdx.x;
+    const int g = G == 1 ? 0 : tid / Z;
+    const int r = tid - g * Z;
+    const long long f0 = (long long)blockIdx.x * G;
+    const long long left = a.frames - f0;
+    const int nf = left < G ? (int)left : G;
+    float* P = smem_post + g * N;
+
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        s_fail[0] = 0;
+        s_fail[1] = 0;
+        const uint32_t bytes = (uint32_t)(nf * N * 4);
+        mbar_arrive_expect_tx(&bar, bytes);
+        bulk_g2s(smem_post, a.llr + f0 * N, bytes, &bar);
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+            atomicOr(a.err, kErrWaitTimeout);
+            mbar_wait_bounded(&bar, 0);   /* let an in-flight copy land before exit */
+        }
+        return;
+    }
+
+    /* syndrome of the current posterior for this thread's rows: 1 if any fails */
+    auto rows_fail = [&]() -> unsigned {
+        unsigned fail = 0;
+        static_for<MB>([&](auto I) {
+            constexpr int d = layer_degree(R, I);
+            uint32_t acc = (uint32_t)(d & 1) << 31;
+            static_for<d>([&](auto E) {
+                acc ^= __float_as_uint(canon(P[edge_var<R, ZT, I, E>(r, a)]));
+            });
+            fail |= acc >> 31;
+        });
+        return fail;
+    };
+    /* per-frame OR over the CTA; returns this frame's flag and whether any
+     * live frame is still failing */
+    auto frame_fail = [&](unsigned fail, int slot, bool& any) -> bool {
+        if constexpr (G == 1) {
+            any = __syncthreads_or((int)fail) != 0;
+            return any;
+        } else {
+            if (fail) atomicOr(&s_fail[slot], 1u << g);
+            __syncthreads();
+            const unsigned m = s_fail[slot];
+            any = m != 0;
+            return (m >> g) & 1u;
+        }
+    };
+
+    const bool live = g < nf;
+    bool any_fail;
+    bool active = frame_fail(live ? rows_fail() : 0u, 0, any_fail);
+    int iters = 0;
+
+    /* compressed messages per layer: magnitudes and NEG = sign bits (bit
+     * d-1-e for edge e) | argmin edge << 27 */
+    float M1[MB], M2[MB];
+    uint32_t NEG[MB];
+#pragma unroll
+    for (int i = 0; i < MB; i++) { M1[i] = 0.0f; M2[i] = 0.0f; NEG[i] = 0u; }
+
+    for (int it = 1; it <= a.max_iter && any_fail; ++it) {
+        if constexpr (G > 1) {
+            if (tid == 0) s_fail[it & 1] = 0;   /* slot it&1 was last read before the previous barrier */
+        }
+        static_for<MB>([&](auto I) {
+            constexpr int d = layer_degree(R, I);
+            if (active) {
+                float L[d];
+                uint32_t sgn = 0;
+                float m1 = 10000.0f, m2 = 10000.0f;
+                const float oM1 = M1[I], oM2 = M2[I];
+                const uint32_t oNeg = NEG[I];
+                const int oIdx = (int)(oNeg >> 27);
+                /* pass 1: L = post - old message, sign bits, two minima */
+                static_for<d>([&](auto E) {
+                    constexpr int e = decltype(E)::value;
+                    const float x = P[edge_var<R, ZT, I, e>(r, a)];
+                    const float mag = (oIdx == e) ? oM2 : oM1;
+                    const uint32_t sb = (oNeg << (32 - d + e)) & 0x80000000u;
+                    const float msg = __uint_as_float(__float_as_uint(mag) | sb);
+                    const float l = __fsub_rn(x, msg);
+                    L[e] = l;
+                    sgn = __funnelshift_l(__float_as_uint(canon(l)), sgn, 1);
+                    const float al = fabsf(l);
+                    m2 = fminf(m2, fmaxf(m1, al));
+                    m1 = fminf(m1, al);
+                });
+                /* bit (d-1-e) of sgn is neg(L_e); message e is negative iff
+                 * (d & 1) ^ parity(neg) ^ neg(L_e)  (reference :148,172,191) */
+                const uint32_t flip = (uint32_t)((d & 1) ^ (__popc(sgn) & 1));
+                const uint32_t dmask = (d >= 32) ? 0xffffffffu : ((1u << d) - 1u);
+                int nIdx = 0;
+                if constexpr (MODE == kMs) {
+                    const uint32_t fb = flip << 31;
+                    static_for<d>([&](auto E) {
+                        constexpr int e = decltype(E)::value;
+                        const float l = L[e];
+                        const bool is_min = fabsf(l) == m1;
+                        const float mu = is_min ? m2 : m1;
+                        nIdx = is_min ? e : nIdx;
+                        const uint32_t sb = ((sgn << (32 - d + e)) & 0x80000000u) ^ fb;
+                        const float t = __uint_as_float(__float_as_uint(mu) | sb);
+                        P[edge_var<R, ZT, I, e>(r, a)] = __fadd_rn(l, t);
+                    });
+                    M1[I] = m1;
+                    M2[I] = m2;
+                } else {
+                    double D1, D2;
+                    if constexpr (MODE == kNms) {
+                        D1 = __dmul_rn((double)m1, 0.815);
+                        D2 = __dmul_rn((double)m2, 0.815);
+                    } else {
+                        const double t1 = __dsub_rn((double)m1, 0.10);
+                        const double t2 = __dsub_rn((double)m2, 0.10);
+                        D1 = t1 < 0.0 ? 0.0 : t1;
+                        D2 = t2 < 0.0 ? 0.0 : t2;
+                    }
+                    const uint32_t fb = flip << 31;
+                    const int h1 = __double2hiint(D1) ^ (int)fb, l1 = __double2loint(D1);
+                    const int h2 = __double2hiint(D2) ^ (int)fb, l2 = __double2loint(D2);
+                    static_for<d>([&](auto E) {
+                        constexpr int e = decltype(E)::value;
+                        const float l = L[e];
+                        const bool is_min = fabsf(l) == m1;
+                        nIdx = is_min ? e : nIdx;
+                        int hi = is_min ? h2 : h1;
+                        const int lo = is_min ? l2 : l1;
+                        hi ^= (int)((sgn << (32 - d + e)) & 0x80000000u);
+                        const double t = __hiloint2double(hi, lo);
+                        P[edge_var<R, ZT, I, e>(r, a)] = __double2float_rn(__dadd_rn((double)l, t));
+                    });
+                    M1[I] = __double2float_rn(D1);
+                    M2[I] = __double2float_rn(D2);
+                }
+                NEG[I] = ((sgn ^ (flip ? dmask : 0u)) & dmask) | ((uint32_t)nIdx << 27);
+            }
+            __syncthreads();
+        });
+        const bool f = frame_fail(live && active ? rows_fail() : 0u, it & 1, any_fail);
+        if (active) {
+            iters = it;
+            active = f;
+        }
+    }
+
+    /* outputs: hard bits and posterior, vectorised over the CTA's frames */
+    const int total = nf * N;
+    int8_t* hard = a.hard + f0 * N;
+    for (int v = tid * 4; v < total; v += nthreads * 4) {
+        const float4 p = *reinterpret_cast<const float4*>(smem_post + v);
+        const uint32_t w = (p.x >= 0.0f ? 1u : 0u) | (p.y >= 0.0f ? 1u << 8 : 0u) |
+                           (p.z >= 0.0f ? 1u << 16 : 0u) | (p.w >= 0.0f ? 1u << 24 : 0u);
+        *reinterpret_cast<uint32_t*>(hard + v) = w;
+        if (a.post) *reinterpret_cast<float4*>(a.post + f0 * N + v) = p;
+    }
+    if (a.status && live && r == 0)
+        a.status[f0 + g] = iters | ((active ? 1 : 0) << 16);
+}
+
+}  // namespace wldpc
+
+#endif
