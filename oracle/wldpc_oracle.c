@@ -411,19 +411,18 @@ static unsigned learned_one(const wo_code_t* c, int T, const float* A, const flo
                 int v[WO_NB];
                 unsigned negpar = 0;
                 float m1 = INFINITY, m2 = INFINITY;
-                int am = 0;
                 for (int e = 0; e < d; e++) {
                     v[e] = var_of(c, b0 + e, r);
                     L[e] = rx[v[e]] - msg[(b0 + e) * z + r];
                     negpar ^= (unsigned)(signbit(L[e]) != 0);
                     float a = fabsf(L[e]);
-                    if (a < m1) { m2 = m1; m1 = a; am = e; }
-                    else if (a < m2) { m2 = a; }
+                    m2 = fminf(m2, fmaxf(m1, a));
+                    m1 = fminf(m1, a);
                 }
                 for (int e = 0; e < d; e++) {
                     unsigned neg_e = (unsigned)(signbit(L[e]) != 0);
                     unsigned negmsg = negpar ^ neg_e;      /* product of the other signs */
-                    float mu = (e == am) ? m2 : m1;
+                    float mu = (fabsf(L[e]) == m1) ? m2 : m1;
                     int col = c->blk_col[b0 + e];
                     float mag = fmaf(A[widx(t, i, col)], mu, -B[widx(t, i, col)]);
                     mag = fmaxf(mag, 0.0f);
@@ -474,6 +473,13 @@ static double sigmoid(double x) { return x >= 0 ? 1.0 / (1.0 + exp(-x)) : exp(x)
 double wo_learned_loss_grad(int rate, int z, int iterations, const float* w, long frames,
                             const float* llr, const uint8_t* cw, double* grad)
 {
+    /* Forward in float with exactly the decoder's operations (so that every
+     * min / argmin / gate decision equals the device's), tape kept, and the
+     * reverse sweep accumulated in double. Subgradients: sign() and the
+     * argmin choice are constants; d|x|/dx = sign(x) with signbit; relu'(0) = 0.
+     * Routing of the min: i1 = first edge with |L| == min1, i2 = first other
+     * edge with |L| == min2; edge e != i1 takes its magnitude from i1, edge i1
+     * from i2. */
     wo_code_t c;
     if (wo_code(rate, z, &c)) return NAN;
     const int T = iterations, n = c.n, E = c.nblk * z;
@@ -483,57 +489,57 @@ double wo_learned_loss_grad(int rate, int z, int iterations, const float* w, lon
     memset(grad, 0, sizeof(double) * 2 * WN);
     const double inv = 1.0 / ((double)T * (double)n * (double)frames);
 
-    double* P = (double*)malloc(sizeof(double) * n);
-    double* msg = (double*)malloc(sizeof(double) * E);
+    float* P = (float*)malloc(sizeof(float) * n);
+    float* msg = (float*)malloc(sizeof(float) * E);
     double* gP = (double*)malloc(sizeof(double) * n);
     double* gm = (double*)malloc(sizeof(double) * E);
-    /* per-iteration tape: L, mu, source edge of mu, sign and gate per edge */
-    double* Lt = (double*)malloc(sizeof(double) * (size_t)T * E);
-    double* mut = (double*)malloc(sizeof(double) * (size_t)T * E);
+    float* Lt = (float*)malloc(sizeof(float) * (size_t)T * E);
+    float* mut = (float*)malloc(sizeof(float) * (size_t)T * E);
     int* srct = (int*)malloc(sizeof(int) * (size_t)T * E);
     signed char* st = (signed char*)malloc((size_t)T * E);
     signed char* gt = (signed char*)malloc((size_t)T * E);
-    double* Pt = (double*)malloc(sizeof(double) * (size_t)T * n);
+    float* Pt = (float*)malloc(sizeof(float) * (size_t)T * n);
     double loss = 0.0;
 
     for (long f = 0; f < frames; f++) {
         const float* lf = llr + f * n;
         const uint8_t* cf = cw + f * n;
-        for (int v = 0; v < n; v++) P[v] = lf[v];
-        memset(msg, 0, sizeof(double) * E);
+        memcpy(P, lf, sizeof(float) * n);
+        memset(msg, 0, sizeof(float) * E);
         for (int t = 0; t < T; t++) {
             for (int i = 0; i < c.mb; i++) {
                 const int b0 = c.row_start[i], d = c.row_start[i + 1] - b0;
                 for (int r = 0; r < z; r++) {
-                    double L[WO_NB];
+                    float L[WO_NB];
                     int v[WO_NB];
-                    int negpar = 0, i1 = -1, i2 = -1;
-                    double m1 = INFINITY, m2 = INFINITY;
+                    unsigned negpar = 0;
+                    float m1 = INFINITY, m2 = INFINITY;
                     for (int e = 0; e < d; e++) {
-                        int eg = (b0 + e) * z + r;
                         v[e] = var_of(&c, b0 + e, r);
-                        L[e] = P[v[e]] - msg[eg];
-                        negpar ^= signbit(L[e]) != 0;
-                        double a = fabs(L[e]);
-                        if (a < m1) { m2 = m1; i2 = i1; m1 = a; i1 = e; }
-                        else if (a < m2) { m2 = a; i2 = e; }
+                        L[e] = P[v[e]] - msg[(b0 + e) * z + r];
+                        negpar ^= (unsigned)(signbit(L[e]) != 0);
+                        float a = fabsf(L[e]);
+                        m2 = fminf(m2, fmaxf(m1, a));
+                        m1 = fminf(m1, a);
                     }
+                    int i1 = 0, i2 = -1;
+                    while (fabsf(L[i1]) != m1) i1++;
+                    for (int e = 0; e < d; e++)
+                        if (e != i1 && fabsf(L[e]) == m2) { i2 = e; break; }
                     for (int e = 0; e < d; e++) {
-                        int eg = (b0 + e) * z + r;
-                        int col = c.blk_col[b0 + e];
-                        int neg = negpar ^ (signbit(L[e]) != 0);
-                        double s = neg ? -1.0 : 1.0;
-                        double mu = (e == i1) ? m2 : m1;
-                        int src = (e == i1) ? i2 : i1;
-                        double pre = (double)A[widx(t, i, col)] * mu - (double)B[widx(t, i, col)];
-                        int gate = pre > 0.0;
-                        double m = s * (gate ? pre : 0.0);
-                        size_t k = (size_t)t * E + eg;
+                        const int eg = (b0 + e) * z + r;
+                        const int col = c.blk_col[b0 + e];
+                        const unsigned neg = negpar ^ (unsigned)(signbit(L[e]) != 0);
+                        const float mu = (fabsf(L[e]) == m1) ? m2 : m1;
+                        const float pre = fmaf(A[widx(t, i, col)], mu, -B[widx(t, i, col)]);
+                        const float mag = fmaxf(pre, 0.0f);
+                        const float m = flip_sign(mag, neg);
+                        const size_t k = (size_t)t * E + eg;
                         Lt[k] = L[e];
                         mut[k] = mu;
-                        srct[k] = (b0 + src) * z + r;
+                        srct[k] = (b0 + ((e == i1) ? i2 : i1)) * z + r;
                         st[k] = (signed char)(neg ? -1 : 1);
-                        gt[k] = (signed char)gate;
+                        gt[k] = (signed char)(pre > 0.0f);
                         msg[eg] = m;
                         P[v[e]] = L[e] + m;
                     }
@@ -541,17 +547,16 @@ double wo_learned_loss_grad(int rate, int z, int iterations, const float* w, lon
             }
             for (int v = 0; v < n; v++) {
                 Pt[(size_t)t * n + v] = P[v];
-                double sg = cf[v] ? -1.0 : 1.0;    /* loss = softplus(sg * P) */
-                loss += softplus(sg * P[v]) * inv;
+                const double sg = cf[v] ? -1.0 : 1.0;      /* loss = softplus(sg * P) */
+                loss += softplus(sg * (double)P[v]) * inv;
             }
         }
-        /* reverse sweep */
         memset(gP, 0, sizeof(double) * n);
         memset(gm, 0, sizeof(double) * E);
         for (int t = T - 1; t >= 0; t--) {
             for (int v = 0; v < n; v++) {
-                double sg = cf[v] ? -1.0 : 1.0;
-                gP[v] += sg * sigmoid(sg * Pt[(size_t)t * n + v]) * inv;
+                const double sg = cf[v] ? -1.0 : 1.0;
+                gP[v] += sg * sigmoid(sg * (double)Pt[(size_t)t * n + v]) * inv;
             }
             for (int i = c.mb - 1; i >= 0; i--) {
                 const int b0 = c.row_start[i], d = c.row_start[i + 1] - b0;
@@ -563,24 +568,23 @@ double wo_learned_loss_grad(int rate, int z, int iterations, const float* w, lon
                         gL[e] = gP[v[e]];
                     }
                     for (int e = 0; e < d; e++) {
-                        int eg = (b0 + e) * z + r;
-                        size_t k = (size_t)t * E + eg;
+                        const int eg = (b0 + e) * z + r;
+                        const size_t k = (size_t)t * E + eg;
                         if (!gt[k]) continue;
-                        int col = c.blk_col[b0 + e];
-                        double G = gP[v[e]] + gm[eg];
-                        double s = (double)st[k];
-                        grad[widx(t, i, col)] += G * s * mut[k];
+                        const int col = c.blk_col[b0 + e];
+                        const double G = gP[v[e]] + gm[eg];
+                        const double s = (double)st[k];
+                        grad[widx(t, i, col)] += G * s * (double)mut[k];
                         grad[WN + widx(t, i, col)] += -G * s;
-                        double gmu = G * s * (double)A[widx(t, i, col)];
-                        int src = srct[k];
-                        int se = src / z - b0;     /* edge position of the source within the row */
-                        double Ls = Lt[(size_t)t * E + src];
+                        const double gmu = G * s * (double)A[widx(t, i, col)];
+                        const int src = srct[k];
+                        const int se = src / z - b0;
+                        const float Ls = Lt[(size_t)t * E + src];
                         gL[se] += gmu * (signbit(Ls) ? -1.0 : 1.0);
                     }
                     for (int e = 0; e < d; e++) {
-                        int eg = (b0 + e) * z + r;
                         gP[v[e]] = gL[e];
-                        gm[eg] = -gL[e];
+                        gm[(b0 + e) * z + r] = -gL[e];
                     }
                 }
             }

@@ -82,16 +82,23 @@ constexpr int block_index(int rate, int i, int e)
     return b + e;
 }
 
+/* variable index of edge E of layer I for row r, z a compile-time constant */
+template <int R, int Z, int I, int E>
+__device__ __forceinline__ int edge_var_c(int r)
+{
+    constexpr int col = layer_col(R, I, E);
+    constexpr int s = layer_shift(R, Z, I, E);
+    int t = r + s;
+    t = (t >= Z) ? t - Z : t;
+    return col * Z + t;
+}
+
 /* variable index of edge E of layer I for row r */
 template <int R, int ZT, int I, int E>
 __device__ __forceinline__ int edge_var(int r, const DecodeArgs& a)
 {
     if constexpr (ZT > 0) {
-        constexpr int col = layer_col(R, I, E);
-        constexpr int s = layer_shift(R, ZT, I, E);
-        int t = r + s;
-        t = (t >= ZT) ? t - ZT : t;
-        return col * ZT + t;
+        return edge_var_c<R, ZT, I, E>(r);
     } else {
         constexpr int b = block_index(R, I, E);
         int t = r + (int)a.shift[b];
@@ -190,6 +197,7 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
             constexpr int d = layer_degree(R, I);
             if (active) {
                 float L[d];
+                uint32_t LC[d];
                 uint32_t sgn = 0;
                 float m1 = 10000.0f, m2 = 10000.0f;
                 const float oM1 = M1[I], oM2 = M2[I];
@@ -204,7 +212,8 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
                     const float msg = __uint_as_float(__float_as_uint(mag) | sb);
                     const float l = __fsub_rn(x, msg);
                     L[e] = l;
-                    sgn = __funnelshift_l(__float_as_uint(canon(l)), sgn, 1);
+                    LC[e] = __float_as_uint(canon(l));
+                    sgn = __funnelshift_l(LC[e], sgn, 1);
                     const float al = fabsf(l);
                     m2 = fminf(m2, fmaxf(m1, al));
                     m1 = fminf(m1, al);
@@ -222,7 +231,7 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
                         const bool is_min = fabsf(l) == m1;
                         const float mu = is_min ? m2 : m1;
                         nIdx = is_min ? e : nIdx;
-                        const uint32_t sb = ((sgn << (32 - d + e)) & 0x80000000u) ^ fb;
+                        const uint32_t sb = (LC[e] & 0x80000000u) ^ fb;
                         const float t = __uint_as_float(__float_as_uint(mu) | sb);
                         P[edge_var<R, ZT, I, e>(r, a)] = __fadd_rn(l, t);
                     });
@@ -249,7 +258,7 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
                         nIdx = is_min ? e : nIdx;
                         int hi = is_min ? h2 : h1;
                         const int lo = is_min ? l2 : l1;
-                        hi ^= (int)((sgn << (32 - d + e)) & 0x80000000u);
+                        hi ^= (int)(LC[e] & 0x80000000u);
                         const double t = __hiloint2double(hi, lo);
                         P[edge_var<R, ZT, I, e>(r, a)] = __double2float_rn(__dadd_rn((double)l, t));
                     });
