@@ -45,6 +45,7 @@ extern "C" {
 #define WLDPC_ERR_NO_DEVICE (-4)    /* no usable CUDA device */
 #define WLDPC_ERR_TIMEOUT (-5)      /* a bounded device-side wait expired */
 #define WLDPC_ERR_UNSUPPORTED (-6)  /* operation not available for this code */
+#define WLDPC_ERR_SCRATCH (-7)      /* request larger than the allocation-free entry point's scratch */
 
 /* Decoder flavours: the reference's compile-time switch (reference
  * lib/ldpc_decoder.cc:17-21), selectable at run time here. */
@@ -172,6 +173,29 @@ WLDPC_API int wldpc_encode_batch_device(wldpc_encoder* enc, const uint8_t* info,
 WLDPC_API int wldpc_framegen_device(int rate, unsigned z, uint64_t seed, uint64_t first_frame, size_t frames,
                           float ebno_lo_db, float ebno_hi_db, uint8_t* info, uint8_t* codeword, float* llr,
                           float* ebno_db, void* stream);
+
+/* ------------------------------------------------- allocation-free decode */
+
+/* Size of the static device scratch used by wldpc_decode_host_noalloc. */
+#define WLDPC_NOALLOC_SCRATCH_BYTES (1u << 20)
+
+/* No counterpart in the reference: an allocation-free form of the batched
+ * host decode, for callers that cannot call cudaMalloc -- hosts whose device
+ * memory is owned by another allocator, real-time threads where an
+ * allocation's device synchronisation is not allowed, and calls that cannot
+ * keep a decoder handle alive. It creates no handle and allocates nothing:
+ * its device scratch is a static 1 MiB array (held by every GPU that loads
+ * the library until the process exits). Semantics are those of
+ * wldpc_decode_batch_host with WLDPC_MODE_NMS: rx_codewords (frames x n host
+ * floats) receives the posterior, decoded the hard bits, num_errors (nullable)
+ * the per-frame reference return values. The staging must fit the scratch
+ * (about 5n bytes per frame: at most 90 frames at z=96, 363 at z=24); larger requests
+ * return WLDPC_ERR_SCRATCH. The first call on a device looks up the scratch
+ * address and should come before any stream capture. All calls share the
+ * scratch: calls that overlap on the GPU race and must be serialised. Runs on
+ * the default stream and returns when the results are in host memory. */
+WLDPC_API int wldpc_decode_host_noalloc(int rate, unsigned z, unsigned max_iter, float* rx_codewords,
+                                        int8_t* decoded, uint32_t* num_errors, size_t frames);
 
 /* ------------------------------------------------------------- BER runner */
 

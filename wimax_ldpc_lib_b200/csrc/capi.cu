@@ -109,6 +109,7 @@ const char* wldpc_strerror(int code)
     case WLDPC_ERR_NO_DEVICE: return "no CUDA device";
     case WLDPC_ERR_TIMEOUT: return "device-side wait timed out";
     case WLDPC_ERR_UNSUPPORTED: return "operation not supported for this code";
+    case WLDPC_ERR_SCRATCH: return "request exceeds the static scratch of the allocation-free entry point";
     default: return "unknown error";
     }
 }
