@@ -5,7 +5,12 @@ seeded synthetic frames (random info bits, the project's encoder, BPSK, AWGN,
 LLR = 2y/sigma^2) generated on the device at Eb/N0 = 2.25 dB, where the plain
 normalized min-sum decoder with the reference's cap of 10 iterations has
 FER <= 1e-3. A step decodes one batch of 262144 frames (2.4 GB of float32 LLRs,
-larger than L2, so no flush is needed between steps).
+larger than L2, so no flush is needed between steps). Both decoders run on the
+same frames: the plain (bit-exact) decoder and, when trained weights are
+shipped, the learned min-sum decoder (8 trained iterations, run to the same
+cap of 10 with the last trained weights); `value` is the learned one's when
+its FER meets the target, is no worse than the plain decoder's and it is
+faster, else the plain one's; `decoders` reports both.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -210,6 +215,9 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+LMS_WEIGHTS = os.path.join(ROOT, "wimax_ldpc_lib_b200", "weights", "lms_r0_z96_T8.json")
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -225,87 +233,116 @@ def run_ours(args):
     wl.framegen_device(RATE, Z, SEED, rank * frames, frames, EBNO_DB, EBNO_DB, info=info, llr=llr)
     hard = torch.empty((frames, n), dtype=torch.int8, device=dev)
     status = torch.empty(frames, dtype=torch.int32, device=dev)
-    dec = wl.Decoder(RATE, Z, MAX_ITER)
     stream = torch.cuda.Stream()
     torch.cuda.synchronize()
 
-    for _ in range(args.warmup):
-        dec.decode_device(llr, hard, None, status, stream=stream)
-    torch.cuda.synchronize()
-    dec.synchronize()
+    decoders = {"plain": wl.Decoder(RATE, Z, MAX_ITER)}
+    lms_meta = None
+    if os.path.exists(LMS_WEIGHTS) and not args.plain_only:
+        with open(LMS_WEIGHTS) as f:
+            lms_meta = json.load(f)
+        # the learned decoder at the reference's cap (iterations past the trained
+        # ones reuse the last trained weights), judged against plain at cap 10
+        decoders["learned"] = wl.LearnedDecoder(RATE, Z, lms_meta["iterations"],
+                                                weights=np.array(lms_meta["weights"], np.float32), cap=MAX_ITER)
+
+    def measure(dec):
+        for _ in range(args.warmup):
+            dec.decode_device(llr, hard, None, status, stream=stream)
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(args.steps):
+            dec.decode_device(llr, hard, None, status, stream=stream)
+        stop.record(stream)
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+        ms = start.elapsed_time(stop) / args.steps
+        ferr = (hard[:, :k].view(torch.uint8) != info).any(dim=1).sum().to(torch.float64)
+        iters = (status & 0xFFFF).to(torch.float64).sum()
+        c = torch.stack([ferr, iters, torch.tensor(ms, dtype=torch.float64, device=dev)])
+        if ws > 1:
+            torch.distributed.all_reduce(c[:2])
+            m = c[2:].clone()
+            torch.distributed.all_reduce(m, op=torch.distributed.ReduceOp.MAX)
+            c[2] = m[0]
+        total = frames * ws
+        ms = float(c[2].item())
+        return {"value": total * k / (ms * 1e-3) / 1e9, "ms_per_step": ms, "fer": float(c[0].item()) / total,
+                "mean_iterations": float(c[1].item()) / total}
 
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    if ws > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    start = torch.cuda.Event(enable_timing=True)
-    stop = torch.cuda.Event(enable_timing=True)
-    start.record(stream)
-    for _ in range(args.steps):
-        dec.decode_device(llr, hard, None, status, stream=stream)
-    stop.record(stream)
-    torch.cuda.synchronize()
-    if ws > 1:
-        torch.distributed.barrier()
+    results = {name: measure(dec) for name, dec in decoders.items()}
     clocks = sampler.stop()
-    dec.synchronize()
-    ms = start.elapsed_time(stop) / args.steps
+    for dec in decoders.values():
+        if hasattr(dec, "synchronize"):
+            dec.synchronize()
 
-    # quality of the last step
-    ferr = (hard[:, :k].view(torch.uint8) != info).any(dim=1).sum()
-    st = status
-    iters = (st & 0xFFFF).to(torch.float64).sum()
-    synfail = ((st >> 16) & 1).sum()
-    counters = torch.stack([ferr.to(torch.float64), iters, synfail.to(torch.float64)])
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        torch.distributed.all_reduce(counters)
-        torch.distributed.all_reduce(ms_t, op=torch.distributed.ReduceOp.MAX)
-    ms = float(ms_t.item())
-    total_frames = frames * ws
-    fer = float(counters[0].item()) / total_frames
-    mean_iters = float(counters[1].item()) / total_frames
-    value = total_frames * k / (ms * 1e-3) / 1e9
+    # the headline decoder: learned where it meets the FER target and is faster, else plain
+    head = "plain"
+    if "learned" in results:
+        L, P = results["learned"], results["plain"]
+        # ships where it meets the target, is no worse than plain and is faster
+        if L["fer"] <= 1e-3 and L["fer"] <= P["fer"] and L["value"] > P["value"]:
+            head = "learned"
+    R = results[head]
+    ms = R["ms_per_step"]
+    value = R["value"]
+    dec = decoders[head]
 
-    # e2e through the C ABI host call (pinned host buffers, copies in the timed region)
+    # e2e through the C ABI host call of the same decoder (pinned host buffers,
+    # copies in the timed region)
     e2e = None
     if not args.no_e2e:
         llr_h = torch.empty((frames, n), dtype=torch.float32, pin_memory=True)
         hard_h = torch.empty((frames, n), dtype=torch.int8, pin_memory=True)
         st_h = torch.empty(frames, dtype=torch.int32, pin_memory=True)
         src = llr.cpu()
+
+        def host_call():
+            if head == "plain":
+                dec.decode_host_into(llr_h, hard_h, None, st_h)
+            else:
+                wl._check(wl.lib().wldpc_lms_decode_host(dec._h, wl._t_ptr(llr_h), wl._t_ptr(hard_h), None,
+                                                         wl._t_ptr(st_h), frames), "lms decode_host")
         e2e_steps = max(1, min(args.steps, 3))
         llr_h.copy_(src)
-        dec.decode_host_into(llr_h, hard_h, None, st_h)        # warm-up
+        host_call()                                            # warm-up
         times = []
         for _ in range(e2e_steps):
             llr_h.copy_(src)                                   # fresh input (decode writes posteriors back)
             torch.cuda.synchronize()
             t = time.perf_counter()
-            dec.decode_host_into(llr_h, hard_h, None, st_h)
+            host_call()
             times.append(time.perf_counter() - t)
-        t_e2e = max(times) if ws == 1 else max(times)
-        t_e2e_t = torch.tensor([sum(times) / len(times)], dtype=torch.float64, device=dev)
+        t_e2e = torch.tensor([sum(times) / len(times)], dtype=torch.float64, device=dev)
         if ws > 1:
-            torch.distributed.all_reduce(t_e2e_t, op=torch.distributed.ReduceOp.MAX)
-        e2e = {"value": total_frames * k / float(t_e2e_t.item()) / 1e9, "unit": "info Gbit/s",
+            torch.distributed.all_reduce(t_e2e, op=torch.distributed.ReduceOp.MAX)
+        e2e = {"value": frames * ws * k / float(t_e2e.item()) / 1e9, "unit": "info Gbit/s",
                "h2d_bytes_per_step": frames * n * 4,
                "d2h_bytes_per_step": frames * n * 4 + frames * n + frames * 4,
-               "api": "wldpc_decode_batch_host (pinned host buffers, posterior + hard bits + status back)",
+               "api": ("wldpc_decode_batch_host" if head == "plain" else "wldpc_lms_decode_host") +
+                      " (pinned host buffers; posterior, hard bits and status copied back)",
                "timing": "host wall clock around the synchronous call, mean of %d" % e2e_steps}
         del llr_h, hard_h, st_h, src
 
     peak, peak_kind = load_peaks()
     bytes_per_launch = frames * 5 * n
     achieved = bytes_per_launch / (ms * 1e-3) / 1e9
-    traffic = load_traffic("tdmp_nms_r12_z96.txt")
+    traffic = load_traffic("tdmp_nms_r12_z96.txt" if head == "plain" else "lms_r12_z96.txt")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_kind": peak_kind,
+                "traffic": traffic, "peak_kind": peak_kind, "kernel": "tdmp_decode_kernel<0,96,NMS>"
+                if head == "plain" else "lms_decode_kernel<0,96>",
                 "algorithmic_bytes_per_launch": bytes_per_launch,
-                "note": "5n bytes per frame (float32 LLR read + int8 hard-decision write); the kernel is "
-                        "issue-bound, not HBM-bound (see DESIGN.md)"}
+                "note": "5n bytes per frame (float32 LLR read + int8 hard-decision write); the decoders are "
+                        "instruction-issue bound, not HBM-bound (see DESIGN.md)"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -313,19 +350,24 @@ def run_ours(args):
         cpu = cpu_reference_baseline(llr[:n_sample].cpu().numpy())
 
     if rank == 0:
+        cfg_dec = {"plain": f"plain NMS TDMP (bit-exact), cap {MAX_ITER}",
+                   "learned": f"learned min-sum ({lms_meta['iterations'] if lms_meta else 8} trained iterations), "
+                              f"cap {MAX_ITER}"}
         line = {"metric": METRIC, "value": value, "unit": "info Gbit/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-                "config": {"workload": f"plain NMS TDMP decode (bit-exact), rate 1/2 z=96, {frames} frames per GPU "
-                                       f"per step, Eb/N0 {EBNO_DB} dB, cap {MAX_ITER}",
-                           "frames_per_gpu": frames, "ebno_db": EBNO_DB, "max_iter": MAX_ITER,
-                           "decoder": "plain", "l2": "inputs larger than L2 (2.4 GB per GPU), no flush",
+                "vs_baseline": None, "dtype": "f32" if head == "learned" else "f32+f64", "data": "synthetic",
+                "config": {"workload": f"{cfg_dec[head]} decode, rate 1/2 z=96, {frames} frames per GPU per step, "
+                                       f"Eb/N0 {EBNO_DB} dB",
+                           "frames_per_gpu": frames, "ebno_db": EBNO_DB, "decoder": head,
+                           "l2": "inputs larger than L2 (2.4 GB per GPU), no flush",
                            "parallelism": f"frames sharded over {ws} GPU(s)"},
-                "fer": fer, "mean_iterations": mean_iters, "fer_ok": fer <= 1e-3,
+                "fer": R["fer"], "mean_iterations": R["mean_iterations"], "fer_ok": R["fer"] <= 1e-3,
+                "decoders": {name: dict(r, unit="info Gbit/s", config=cfg_dec[name]) for name, r in results.items()},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": args.steps, "clocks": clocks}
         print(json.dumps(line))
-    dec.close()
+    for d in decoders.values():
+        d.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
 
@@ -339,6 +381,7 @@ def main():
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-only", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -174,6 +174,44 @@ WLDPC_API int wldpc_framegen_device(int rate, unsigned z, uint64_t seed, uint64_
                           float ebno_lo_db, float ebno_hi_db, uint8_t* info, uint8_t* codeword, float* llr,
                           float* ebno_db, void* stream);
 
+/* ----------------------------------------------------- learned min-sum */
+
+/* The learned (neural) normalized/offset min-sum decoder. It generalises the
+ * reference's compile-time NMS/OMS constants (reference
+ * lib/ldpc_decoder.cc:17-21,220-231) to a scale a and an offset b per
+ * (iteration, layer, base column): message = s * max(a*min - b, 0), fp32,
+ * same layered schedule and stopping rule, at most 8 iterations. Weights are
+ * trained on the GPU by the library's own forward/backward kernels and Adam.
+ * Weight tables are float[2][T][12][24]: a then b, [iteration][layer][column];
+ * entries of all-zero blocks are ignored (returned as 0). Supported codes:
+ * every rate at z = 24, 48, 96 (WLDPC_ERR_UNSUPPORTED otherwise); training
+ * needs an encoder, so not rate 3/4B. A new handle starts at a = 0.815, b = 0. */
+typedef struct wldpc_lms wldpc_lms;
+WLDPC_API int wldpc_lms_create(int rate, unsigned z, unsigned iterations, wldpc_lms** out);
+WLDPC_API int wldpc_lms_destroy(wldpc_lms* h);
+WLDPC_API int wldpc_lms_set_weights(wldpc_lms* h, const float* table);
+WLDPC_API int wldpc_lms_get_weights(wldpc_lms* h, float* table);
+/* Iteration cap of decoding (default: the trained iterations T); iterations
+ * past T use the weights of iteration T-1. */
+WLDPC_API int wldpc_lms_set_cap(wldpc_lms* h, unsigned cap);
+/* Decode on device buffers (layout and status as wldpc_decode_batch_device). */
+WLDPC_API int wldpc_lms_decode_device(wldpc_lms* h, const float* llr, int8_t* decoded, float* posterior,
+                                      int32_t* status, size_t frames, void* stream);
+/* Decode host buffers (posterior written back; num_errors = syndrome failed). */
+WLDPC_API int wldpc_lms_decode_host(wldpc_lms* h, float* rx_codewords, int8_t* decoded, uint32_t* num_errors,
+                                    int32_t* status, size_t frames);
+/* Training loss (mean BCE over iterations, bits and frames; positive LLR =
+ * bit 1) and its gradient table for host frames (llr, transmitted codeword
+ * bits 0/1). Synchronous. */
+WLDPC_API int wldpc_lms_loss_grad(wldpc_lms* h, const float* llr, const uint8_t* codeword, size_t frames,
+                                  float* grad_table, double* loss);
+/* `steps` Adam steps (lr, beta 0.9 / 0.999) on batches of `batch` frames
+ * generated on the device (wldpc_framegen_device, Eb/N0 uniform in
+ * [ebno_lo_db, ebno_hi_db], frame counter first_frame + step * batch).
+ * loss_history (nullable) receives the batch loss of every step. */
+WLDPC_API int wldpc_lms_train(wldpc_lms* h, unsigned steps, unsigned batch, float ebno_lo_db, float ebno_hi_db,
+                              uint64_t seed, uint64_t first_frame, float lr, float* loss_history);
+
 /* ------------------------------------------------- allocation-free decode */
 
 /* Size of the static device scratch used by wldpc_decode_host_noalloc. */
@@ -196,6 +234,57 @@ WLDPC_API int wldpc_framegen_device(int rate, unsigned z, uint64_t seed, uint64_
  * the default stream and returns when the results are in host memory. */
 WLDPC_API int wldpc_decode_host_noalloc(int rate, unsigned z, unsigned max_iter, float* rx_codewords,
                                         int8_t* decoded, uint32_t* num_errors, size_t frames);
+
+/* Replaces BER_runner's info-bit source (reference lib/BER_runner.cc:124-146:
+ * LFSR x^31 + x^28 + 1 from 0xdeadbeef, restarted every 115200 bits) on the
+ * device: out[j] = bit first_bit + j of that stream (0/1 bytes). A
+ * BER_runner's frame f uses bits [f*k, (f+1)*k). Asynchronous on stream. */
+WLDPC_API int wldpc_lfsr_bits_device(uint64_t first_bit, size_t nbits, uint8_t* out, void* stream);
+
+/* Seeded random codewords of any code, 3/4B included (which has no
+ * dual-diagonal encoder): uniform over the null space of H (free bits from
+ * Philox stream 0 of (seed, frame), pivot bits from the reduced row-echelon
+ * form computed once per (rate, z) on the host), then the same BPSK / AWGN /
+ * LLR model as wldpc_framegen_device. codeword (frames x n) and llr
+ * (frames x n, 16-byte aligned) and ebno_db may be NULL. Asynchronous. */
+WLDPC_API int wldpc_framegen_nullspace_device(int rate, unsigned z, uint64_t seed, uint64_t first_frame,
+                                              size_t frames, float ebno_lo_db, float ebno_hi_db, uint8_t* codeword,
+                                              float* llr, float* ebno_db, void* stream);
+
+/* --------------------------------------------- mixed-code persistent decode */
+
+/* Code index used by the mixed decoder: rate * 19 + (z - 24) / 4, or
+ * WLDPC_ERR_CODE. */
+WLDPC_API int wldpc_variant(int rate, unsigned z);
+
+/* A batch whose frames use different codes (any rate, any z), decoded by one
+ * persistent launch: frames are binned by code on the device, CTAs take work
+ * items (up to `chunk` frames of one code) from a queue and refill a frame
+ * slot as soon as its frame stops (early-exit compaction). Arithmetic, outputs
+ * and status are those of wldpc_decode_batch_device with WLDPC_MODE_NMS
+ * (bit-exact with the reference). The binning and decode launches are
+ * captured in a CUDA graph on the first call and replayed by later calls with
+ * the same pointers, frame count and configuration. No counterpart in the
+ * reference, whose decoder object handles one code. */
+typedef struct wldpc_mixed wldpc_mixed;
+WLDPC_API int wldpc_mixed_create(unsigned max_iter, wldpc_mixed** out);
+WLDPC_API int wldpc_mixed_destroy(wldpc_mixed* h);
+/* variant[f]: code of frame f; offset[f]: element offset of frame f's n values
+ * in llr / decoded / posterior (frames may be in any order). Asynchronous on
+ * stream (ordered with it through events). */
+WLDPC_API int wldpc_mixed_decode_device(wldpc_mixed* h, const uint8_t* variant, const int64_t* offset,
+                                        const float* llr, int8_t* decoded, float* posterior, int32_t* status,
+                                        size_t frames, void* stream);
+/* Waits for the handle's work; WLDPC_ERR_ARG if a frame had an invalid code. */
+WLDPC_API int wldpc_mixed_synchronize(wldpc_mixed* h);
+/* The autotuner's knobs: CTA size (96 or 192 threads, which sets the frame
+ * slots per CTA to threads / z) and frames per work item. */
+WLDPC_API int wldpc_mixed_set_config(wldpc_mixed* h, int threads, int chunk);
+WLDPC_API int wldpc_mixed_get_config(wldpc_mixed* h, int* threads, int* chunk);
+/* Times every (threads, chunk) candidate on the given batch (repeats launches
+ * each) and keeps the fastest; *best_ms (nullable) gets its time. */
+WLDPC_API int wldpc_mixed_autotune(wldpc_mixed* h, const uint8_t* variant, const int64_t* offset, const float* llr,
+                                   int8_t* decoded, size_t frames, int repeats, float* best_ms);
 
 /* ------------------------------------------------------------- BER runner */
 

@@ -83,7 +83,7 @@ class Oracle:
         L.wo_philox4x32_10.argtypes = [_p, _p, _p]
         L.wo_framegen.argtypes = [_i, _i, ctypes.c_uint64, ctypes.c_uint64, _l, ctypes.c_double,
                                   ctypes.c_double, _p, _p, _p, _p]
-        L.wo_learned_decode_batch.argtypes = [_i, _i, _i, _p, _l, _p, _p, _p, _p, _i]
+        L.wo_learned_decode_batch.argtypes = [_i, _i, _i, _i, _p, _l, _p, _p, _p, _p, _i]
         L.wo_learned_loss_grad.argtypes = [_i, _i, _i, _p, _l, _p, _p, _p]
         L.wo_learned_loss_grad.restype = ctypes.c_double
         self.threads = os.cpu_count() or 1
@@ -175,14 +175,15 @@ class Oracle:
             raise ValueError("wo_framegen failed")
         return info, cw, llr, eb
 
-    def learned_decode(self, rate, z, iterations, w, llr, threads=None):
+    def learned_decode(self, rate, z, iterations, w, llr, threads=None, cap=None):
         llr = np.ascontiguousarray(llr, np.float32)
         w = np.ascontiguousarray(w, np.float32)
         post = llr.copy()
         dec = np.empty(llr.shape, np.int8)
         it = np.empty(llr.shape[0], np.int32)
         sf = np.empty(llr.shape[0], np.int32)
-        if self.lib.wo_learned_decode_batch(rate, z, iterations, _ptr(w), llr.shape[0], _ptr(post),
+        if self.lib.wo_learned_decode_batch(rate, z, iterations, iterations if cap is None else cap, _ptr(w),
+                                            llr.shape[0], _ptr(post),
                                             _ptr(dec), _ptr(it), _ptr(sf), threads or self.threads):
             raise ValueError("wo_learned_decode_batch failed")
         return post, dec, it, sf

@@ -392,7 +392,7 @@ static inline float flip_sign(float x, unsigned neg)
     return v.f;
 }
 
-static unsigned learned_one(const wo_code_t* c, int T, const float* A, const float* B, float* rx,
+static unsigned learned_one(const wo_code_t* c, int T, int cap, const float* A, const float* B, float* rx,
                             int8_t* out, float* msg, int32_t* iters, int32_t* synfail)
 {
     const int z = c->z;
@@ -403,7 +403,8 @@ static unsigned learned_one(const wo_code_t* c, int T, const float* A, const flo
         return 0;
     }
     memset(msg, 0, sizeof(float) * (size_t)c->nblk * z);
-    for (int t = 0; t < T; t++) {
+    for (int it = 0; it < cap; it++) {
+        const int t = it < T ? it : T - 1;     /* past T: the last trained iteration's weights */
         for (int i = 0; i < c->mb; i++) {
             const int b0 = c->row_start[i], d = c->row_start[i + 1] - b0;
             for (int r = 0; r < z; r++) {
@@ -421,7 +422,8 @@ static unsigned learned_one(const wo_code_t* c, int T, const float* A, const flo
                 }
                 for (int e = 0; e < d; e++) {
                     unsigned neg_e = (unsigned)(signbit(L[e]) != 0);
-                    unsigned negmsg = negpar ^ neg_e;      /* product of the other signs */
+                    /* positive LLR = bit 1: the extrinsic sign flips on odd-degree rows */
+                    unsigned negmsg = negpar ^ neg_e ^ (unsigned)(d & 1);
                     float mu = (fabsf(L[e]) == m1) ? m2 : m1;
                     int col = c->blk_col[b0 + e];
                     float mag = fmaf(A[widx(t, i, col)], mu, -B[widx(t, i, col)]);
@@ -434,23 +436,23 @@ static unsigned learned_one(const wo_code_t* c, int T, const float* A, const flo
         }
         slice(rx, out, c->n);
         if (syndrome_one(c, out, 1) == 0) {
-            if (iters) *iters = t + 1;
+            if (iters) *iters = it + 1;
             if (synfail) *synfail = 0;
             return 0;
         }
     }
-    if (iters) *iters = T;
+    if (iters) *iters = cap;
     if (synfail) *synfail = 1;
     return 1;
 }
 
-int wo_learned_decode_batch(int rate, int z, int iterations, const float* w, long frames,
+int wo_learned_decode_batch(int rate, int z, int iterations, int cap, const float* w, long frames,
                             float* llr, int8_t* decoded, int32_t* iters, int32_t* synfail,
                             int threads)
 {
     wo_code_t c;
     if (wo_code(rate, z, &c)) return -1;
-    if (iterations < 1 || iterations > 8) return -1;
+    if (iterations < 1 || iterations > 8 || cap < 0) return -1;
     const float* A = w;
     const float* B = w + (size_t)iterations * WO_L * WO_NB;
     if (threads < 1) threads = 1;
@@ -459,7 +461,7 @@ int wo_learned_decode_batch(int rate, int z, int iterations, const float* w, lon
         float* msg = (float*)malloc(sizeof(float) * (size_t)c.nblk * z);
         #pragma omp for schedule(dynamic, 16)
         for (long f = 0; f < frames; f++)
-            learned_one(&c, iterations, A, B, llr + f * c.n, decoded + f * c.n, msg,
+            learned_one(&c, iterations, cap, A, B, llr + f * c.n, decoded + f * c.n, msg,
                         iters ? iters + f : NULL, synfail ? synfail + f : NULL);
         free(msg);
     }
@@ -510,7 +512,7 @@ double wo_learned_loss_grad(int rate, int z, int iterations, const float* w, lon
             for (int i = 0; i < c.mb; i++) {
                 const int b0 = c.row_start[i], d = c.row_start[i + 1] - b0;
                 for (int r = 0; r < z; r++) {
-                    float L[WO_NB];
+                    float L[WO_NB] = {0};
                     int v[WO_NB];
                     unsigned negpar = 0;
                     float m1 = INFINITY, m2 = INFINITY;
@@ -529,7 +531,7 @@ double wo_learned_loss_grad(int rate, int z, int iterations, const float* w, lon
                     for (int e = 0; e < d; e++) {
                         const int eg = (b0 + e) * z + r;
                         const int col = c.blk_col[b0 + e];
-                        const unsigned neg = negpar ^ (unsigned)(signbit(L[e]) != 0);
+                        const unsigned neg = negpar ^ (unsigned)(signbit(L[e]) != 0) ^ (unsigned)(d & 1);
                         const float mu = (fabsf(L[e]) == m1) ? m2 : m1;
                         const float pre = fmaf(A[widx(t, i, col)], mu, -B[widx(t, i, col)]);
                         const float mag = fmaxf(pre, 0.0f);

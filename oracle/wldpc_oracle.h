@@ -86,9 +86,10 @@ int wo_framegen(int rate, int z, uint64_t seed, uint64_t first_frame, long frame
 
 /* Learned min-sum, float inference: decoder with per-(iteration, layer,
  * block column) scale a and offset b, message = s * max(a*mu - b, 0)
- * (fmaf), min tracking from +inf, early exit on syndrome, cap = iterations.
+ * (fmaf), min tracking from +inf, early exit on syndrome, at most cap
+ * iterations (iterations past `iterations` use the last row of weights).
  * w has 2*iterations*12*24 floats: a then b, each [iteration][layer][col]. */
-int wo_learned_decode_batch(int rate, int z, int iterations, const float* w, long frames,
+int wo_learned_decode_batch(int rate, int z, int iterations, int cap, const float* w, long frames,
                             float* llr, int8_t* decoded, int32_t* iters, int32_t* synfail,
                             int threads);
 /* Learned min-sum training step reference in double precision: loss

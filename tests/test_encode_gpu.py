@@ -53,3 +53,13 @@ def test_framegen_matches_oracle(wl, cuda, oracle, rate):
         l = llr.cpu().numpy().astype(np.float64)
         tol = 2e-5 * np.maximum(1.0, np.abs(ol)) + 1e-4
         assert (np.abs(l - ol) <= tol).all()
+
+
+def test_lfsr_stream_matches_reference_generator(wl, cuda, oracle):
+    torch = cuda
+    ref, _, _ = oracle.lfsr(3 * 115200 + 777)
+    for first in (0, 1152 * 7, 115200 - 100, 2 * 115200 + 5):
+        out = torch.empty(5000, dtype=torch.uint8, device="cuda")
+        wl.lfsr_bits_device(first, out)
+        torch.cuda.synchronize()
+        assert (out.cpu().numpy() == ref[first:first + 5000]).all(), first

@@ -79,6 +79,28 @@ def _lib():
     L.wldpc_encode_batch_device.argtypes = [_p, _p, _p, _sz, _p]
     L.wldpc_framegen_device.argtypes = [_i, _u, ctypes.c_uint64, ctypes.c_uint64, _sz, ctypes.c_float,
                                         ctypes.c_float, _p, _p, _p, _p, _p]
+    L.wldpc_lms_create.argtypes = [_i, _u, _u, ctypes.POINTER(_p)]
+    L.wldpc_lms_destroy.argtypes = [_p]
+    L.wldpc_lms_set_weights.argtypes = [_p, _p]
+    L.wldpc_lms_get_weights.argtypes = [_p, _p]
+    L.wldpc_lms_decode_device.argtypes = [_p, _p, _p, _p, _p, _sz, _p]
+    L.wldpc_lms_set_cap.argtypes = [_p, _u]
+    L.wldpc_lms_decode_host.argtypes = [_p, _p, _p, _p, _p, _sz]
+    L.wldpc_lms_loss_grad.argtypes = [_p, _p, _p, _sz, _p, ctypes.POINTER(ctypes.c_double)]
+    L.wldpc_lms_train.argtypes = [_p, _u, _u, ctypes.c_float, ctypes.c_float, ctypes.c_uint64, ctypes.c_uint64,
+                                  ctypes.c_float, _p]
+    L.wldpc_decode_host_noalloc.argtypes = [_i, _u, _u, _p, _p, _p, _sz]
+    L.wldpc_lfsr_bits_device.argtypes = [ctypes.c_uint64, _sz, _p, _p]
+    L.wldpc_framegen_nullspace_device.argtypes = [_i, _u, ctypes.c_uint64, ctypes.c_uint64, _sz, ctypes.c_float,
+                                                  ctypes.c_float, _p, _p, _p, _p]
+    L.wldpc_variant.argtypes = [_i, _u]
+    L.wldpc_mixed_create.argtypes = [_u, ctypes.POINTER(_p)]
+    L.wldpc_mixed_destroy.argtypes = [_p]
+    L.wldpc_mixed_decode_device.argtypes = [_p, _p, _p, _p, _p, _p, _p, _sz, _p]
+    L.wldpc_mixed_synchronize.argtypes = [_p]
+    L.wldpc_mixed_set_config.argtypes = [_p, _i, _i]
+    L.wldpc_mixed_get_config.argtypes = [_p, ctypes.POINTER(_i), ctypes.POINTER(_i)]
+    L.wldpc_mixed_autotune.argtypes = [_p, _p, _p, _p, _p, _sz, _i, ctypes.POINTER(ctypes.c_float)]
     L.wldpc_ber_runner_create.argtypes = [_i, _u, _u, _u, ctypes.POINTER(_p)]
     L.wldpc_ber_runner_destroy.argtypes = [_p]
     L.wldpc_ber_runner_run_iteration.argtypes = [_p, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]
@@ -246,6 +268,144 @@ def framegen_device(rate, z, seed, first_frame, frames, ebno_lo, ebno_hi=None, i
     _check(_lib().wldpc_framegen_device(rate, z, seed, first_frame, frames, ebno_lo, ebno_hi, _t_ptr(info),
                                         _t_ptr(codeword), _t_ptr(llr), _t_ptr(ebno), _stream_ptr(stream)),
            "framegen")
+
+
+def framegen_nullspace_device(rate, z, seed, first_frame, frames, ebno_lo, ebno_hi=None, codeword=None, llr=None,
+                              ebno=None, stream=None):
+    """Random codewords from the null space of H (any rate, 3/4B included) with AWGN LLRs."""
+    ebno_hi = ebno_lo if ebno_hi is None else ebno_hi
+    _check(_lib().wldpc_framegen_nullspace_device(rate, z, seed, first_frame, frames, ebno_lo, ebno_hi,
+                                                  _t_ptr(codeword), _t_ptr(llr), _t_ptr(ebno), _stream_ptr(stream)),
+           "framegen_nullspace")
+
+
+def variant(rate: int, z: int) -> int:
+    v = _lib().wldpc_variant(rate, z)
+    _check(min(v, 0), "variant")
+    return v
+
+
+class MixedDecoder:
+    """wldpc_mixed handle: one graph launch decodes frames of any mix of codes."""
+
+    def __init__(self, max_iter: int = 10):
+        h = ctypes.c_void_p()
+        _check(_lib().wldpc_mixed_create(max_iter, ctypes.byref(h)), "mixed decoder")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib().wldpc_mixed_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def decode_device(self, variants, offsets, llr, decoded, posterior=None, status=None, stream=None):
+        _check(_lib().wldpc_mixed_decode_device(self._h, _t_ptr(variants), _t_ptr(offsets), _t_ptr(llr),
+                                                _t_ptr(decoded), _t_ptr(posterior), _t_ptr(status),
+                                                variants.numel(), _stream_ptr(stream)), "mixed decode")
+
+    def synchronize(self):
+        _check(_lib().wldpc_mixed_synchronize(self._h), "mixed synchronize")
+
+    def set_config(self, threads: int, chunk: int):
+        _check(_lib().wldpc_mixed_set_config(self._h, threads, chunk), "mixed config")
+
+    def config(self):
+        t, c = _i(), _i()
+        _check(_lib().wldpc_mixed_get_config(self._h, ctypes.byref(t), ctypes.byref(c)), "mixed config")
+        return t.value, c.value
+
+    def autotune(self, variants, offsets, llr, decoded, repeats: int = 3) -> float:
+        ms = ctypes.c_float()
+        _check(_lib().wldpc_mixed_autotune(self._h, _t_ptr(variants), _t_ptr(offsets), _t_ptr(llr), _t_ptr(decoded),
+                                           variants.numel(), repeats, ctypes.byref(ms)), "mixed autotune")
+        return ms.value
+
+
+def lfsr_bits_device(first_bit: int, out, stream=None) -> None:
+    """The reference BER_runner's info-bit stream from position first_bit into a uint8 CUDA tensor."""
+    _check(_lib().wldpc_lfsr_bits_device(first_bit, out.numel(), _t_ptr(out), _stream_ptr(stream)), "lfsr")
+
+
+class LearnedDecoder:
+    """wldpc_lms handle: learned normalized/offset min-sum (weights per
+    iteration, layer and base column), its training and inference."""
+
+    def __init__(self, rate: int, z: int, iterations: int = 8, weights=None, cap: int | None = None):
+        self.rate, self.z, self.iterations = rate, z, iterations
+        self.info = code_info(rate, z)
+        self.n, self.k = self.info.n, self.info.k
+        h = ctypes.c_void_p()
+        _check(_lib().wldpc_lms_create(rate, z, iterations, ctypes.byref(h)), "learned decoder")
+        self._h = h
+        if weights is not None:
+            self.set_weights(weights)
+        if cap is not None:
+            self.set_cap(cap)
+
+    def set_cap(self, cap: int) -> None:
+        """Iteration cap; iterations past the trained ones reuse the last iteration's weights."""
+        _check(_lib().wldpc_lms_set_cap(self._h, cap), "set_cap")
+        self.cap = cap
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib().wldpc_lms_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def table_shape(self):
+        return (2, self.iterations, 12, 24)
+
+    def get_weights(self) -> np.ndarray:
+        t = np.zeros(self.table_shape, np.float32)
+        _check(_lib().wldpc_lms_get_weights(self._h, _np_ptr(t)), "get_weights")
+        return t
+
+    def set_weights(self, table) -> None:
+        t = np.ascontiguousarray(table, np.float32).reshape(self.table_shape)
+        _check(_lib().wldpc_lms_set_weights(self._h, _np_ptr(t)), "set_weights")
+
+    def decode_device(self, llr, decoded, posterior=None, status=None, stream=None):
+        _check(_lib().wldpc_lms_decode_device(self._h, _t_ptr(llr), _t_ptr(decoded), _t_ptr(posterior),
+                                              _t_ptr(status), llr.shape[0], _stream_ptr(stream)), "lms decode")
+
+    def decode_host(self, llr: np.ndarray):
+        post = np.ascontiguousarray(llr, np.float32).copy()
+        frames = post.shape[0]
+        dec = np.empty(post.shape, np.int8)
+        ne = np.empty(frames, np.uint32)
+        st = np.empty(frames, np.int32)
+        _check(_lib().wldpc_lms_decode_host(self._h, _np_ptr(post), _np_ptr(dec), _np_ptr(ne), _np_ptr(st), frames),
+               "lms decode_host")
+        return post, dec, ne, st
+
+    def loss_grad(self, llr: np.ndarray, codeword: np.ndarray):
+        l = np.ascontiguousarray(llr, np.float32)
+        c = np.ascontiguousarray(codeword, np.uint8)
+        g = np.zeros(self.table_shape, np.float32)
+        loss = ctypes.c_double()
+        _check(_lib().wldpc_lms_loss_grad(self._h, _np_ptr(l), _np_ptr(c), l.shape[0], _np_ptr(g),
+                                          ctypes.byref(loss)), "lms loss_grad")
+        return loss.value, g
+
+    def train(self, steps: int, batch: int, ebno_lo: float, ebno_hi: float, seed: int, first_frame: int = 0,
+              lr: float = 1e-3) -> np.ndarray:
+        hist = np.zeros(max(steps, 1), np.float32)
+        _check(_lib().wldpc_lms_train(self._h, steps, batch, ebno_lo, ebno_hi, seed, first_frame, lr,
+                                      _np_ptr(hist)), "lms train")
+        return hist[:steps]
 
 
 class BERRunner:

@@ -10,6 +10,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <random>
 #include <vector>
@@ -440,6 +442,144 @@ int wldpc_framegen_device(int rate, unsigned z, uint64_t seed, uint64_t first_fr
     a.llr = llr;
     a.ebno_out = ebno_db;
     CU(launch_framegen(make_code_desc(rate, (int)z), a, (cudaStream_t)stream));
+    return WLDPC_OK;
+}
+
+/* --------------------------------------------- null-space frame generator */
+
+namespace {
+
+/* H in reduced row-echelon form over GF(2): pivot columns, free columns and
+ * the pivot rows restricted to the free columns, packed; on the device. */
+struct Nullspace {
+    DevBuf A, piv, fre;
+    int rank = 0, nfree = 0, words = 0;
+};
+
+std::mutex g_ns_mutex;
+std::map<int, Nullspace*> g_ns;
+
+int nullspace_for(int rate, int z, Nullspace** out)
+{
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    const int key = (dev * kRates + rate) * 128 + z;
+    std::lock_guard<std::mutex> lock(g_ns_mutex);
+    auto it = g_ns.find(key);
+    if (it != g_ns.end()) {
+        *out = it->second;
+        return WLDPC_OK;
+    }
+    const CodeDesc c = make_code_desc(rate, z);
+    const int n = c.n, m = c.m, W = (n + 31) / 32;
+    std::vector<uint32_t> H((size_t)m * W, 0u);
+    for (int i = 0; i < c.mb; i++)
+        for (int r = 0; r < z; r++)
+            for (int b = c.row_start[i]; b < c.row_start[i + 1]; b++) {
+                int t = r + c.shift[b];
+                t = t >= z ? t - z : t;
+                const int v = c.col[b] * z + t;
+                H[(size_t)(i * z + r) * W + (v >> 5)] ^= 1u << (v & 31);
+            }
+    std::vector<int> pivots;
+    std::vector<char> is_pivot(n, 0);
+    int pr = 0;
+    for (int col = 0; col < n && pr < m; col++) {
+        int sel = -1;
+        for (int r = pr; r < m; r++)
+            if ((H[(size_t)r * W + (col >> 5)] >> (col & 31)) & 1u) { sel = r; break; }
+        if (sel < 0) continue;
+        if (sel != pr)
+            for (int q = 0; q < W; q++) std::swap(H[(size_t)sel * W + q], H[(size_t)pr * W + q]);
+        for (int r = 0; r < m; r++)
+            if (r != pr && ((H[(size_t)r * W + (col >> 5)] >> (col & 31)) & 1u))
+                for (int q = 0; q < W; q++) H[(size_t)r * W + q] ^= H[(size_t)pr * W + q];
+        pivots.push_back(col);
+        is_pivot[col] = 1;
+        pr++;
+    }
+    std::vector<unsigned short> fre;
+    for (int col = 0; col < n; col++)
+        if (!is_pivot[col]) fre.push_back((unsigned short)col);
+    Nullspace* ns = new Nullspace();
+    ns->rank = pr;
+    ns->nfree = (int)fre.size();
+    ns->words = (ns->nfree + 31) / 32;
+    std::vector<uint32_t> A((size_t)pr * ns->words, 0u);
+    for (int i = 0; i < pr; i++)
+        for (int j = 0; j < ns->nfree; j++)
+            if ((H[(size_t)i * W + (fre[j] >> 5)] >> (fre[j] & 31)) & 1u) A[(size_t)i * ns->words + (j >> 5)] |= 1u << (j & 31);
+    std::vector<unsigned short> piv(pivots.begin(), pivots.end());
+    if (ns->A.reserve(A.size() * 4 + 4) || ns->piv.reserve(piv.size() * 2 + 2) || ns->fre.reserve(fre.size() * 2 + 2) ||
+        cudaMemcpy(ns->A.p, A.data(), A.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(ns->piv.p, piv.data(), piv.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(ns->fre.p, fre.data(), fre.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        delete ns;
+        return WLDPC_ERR_CUDA;
+    }
+    g_ns[key] = ns;
+    *out = ns;
+    return WLDPC_OK;
+}
+
+}  // namespace
+
+int wldpc_framegen_nullspace_device(int rate, unsigned z, uint64_t seed, uint64_t first_frame, size_t frames,
+                                    float ebno_lo_db, float ebno_hi_db, uint8_t* codeword, float* llr, float* ebno_db,
+                                    void* stream)
+{
+    if (!valid_rate(rate) || !valid_z((int)z)) return WLDPC_ERR_CODE;
+    if (!aligned(codeword, 4) || !aligned(llr, 16) || !aligned(ebno_db, 4)) return WLDPC_ERR_ARG;
+    int rc = check_device();
+    if (rc) return rc;
+    Nullspace* ns = nullptr;
+    if ((rc = nullspace_for(rate, (int)z, &ns))) return rc;
+    FramegenArgs a;
+    a.seed = seed;
+    a.first_frame = first_frame;
+    a.frames = (long long)frames;
+    a.ebno_lo = ebno_lo_db;
+    a.ebno_hi = ebno_hi_db;
+    a.info = nullptr;
+    a.cw = codeword;
+    a.llr = llr;
+    a.ebno_out = ebno_db;
+    NullspaceArgs na;
+    na.A = (const uint32_t*)ns->A.p;
+    na.pivot_col = (const unsigned short*)ns->piv.p;
+    na.free_col = (const unsigned short*)ns->fre.p;
+    na.rank = ns->rank;
+    na.nfree = ns->nfree;
+    na.words = ns->words;
+    CU(launch_framegen_nullspace(make_code_desc(rate, (int)z), a, na, (cudaStream_t)stream));
+    return WLDPC_OK;
+}
+
+/* ------------------------------------------------------- LFSR info bits */
+
+int wldpc_lfsr_bits_device(uint64_t first_bit, size_t nbits, uint8_t* out, void* stream)
+{
+    if (nbits && !out) return WLDPC_ERR_ARG;
+    int rc = check_device();
+    if (rc) return rc;
+    static bool uploaded[64] = {false};
+    int dev = 0;
+    CU(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return WLDPC_ERR_UNSUPPORTED;
+    if (!uploaded[dev]) {
+        /* one period of the stream, as BER_runner::lfsr_get_num produces it */
+        std::vector<uint32_t> words(115200 / 32, 0u);
+        uint32_t s = 0xdeadbeefu;
+        for (unsigned i = 0; i < 115200; i++) {
+            const uint32_t bit = (s ^ (s >> 3)) & 1u;
+            s = (s >> 1) | (bit << 30);
+            words[i >> 5] |= bit << (i & 31);
+        }
+        CU(upload_lfsr_period(words.data()));
+        uploaded[dev] = true;
+    }
+    CU(launch_lfsr_bits((unsigned long long)first_bit, (long long)nbits, out, (cudaStream_t)stream));
     return WLDPC_OK;
 }
 

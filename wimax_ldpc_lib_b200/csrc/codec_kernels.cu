@@ -38,6 +38,52 @@ __device__ __forceinline__ void philox_at(uint64_t seed, uint64_t frame, uint32_
 
 __device__ __forceinline__ float unif24(uint32_t x) { return ((float)(x >> 8) + 0.5f) * (1.0f / 16777216.0f); }
 
+
+/* BPSK bit*2-1 (positive = bit 1), AWGN from Philox stream 1 by Box-Muller,
+ * LLR = 2y/sigma^2, four code bits per Philox block; bits4(j) returns code
+ * bits j..j+3 in its low 4 bits. */
+template <typename Bits4>
+__device__ __forceinline__ void emit_llr(const CodeDesc& c, const FramegenArgs& a, long long f, uint64_t g, float scale,
+                                         float sigma, int lane, Bits4 bits4)
+{
+    float4* l4 = reinterpret_cast<float4*>(a.llr + f * c.n);
+    for (int j = lane * 4; j < c.n; j += 128) {
+        const uint32_t bits = bits4(j);
+        uint32_t o[4];
+        philox_at(a.seed, g, (uint32_t)(j >> 2), 1u, o);
+        float nrm[4];
+#pragma unroll
+        for (int p = 0; p < 2; p++) {
+            const float u1 = unif24(o[2 * p]), u2 = unif24(o[2 * p + 1]);
+            const float rad = sqrtf(-2.0f * logf(u1));
+            float sn, cs;
+            sincospif(2.0f * u2, &sn, &cs);
+            nrm[2 * p] = rad * cs;
+            nrm[2 * p + 1] = rad * sn;
+        }
+        float4 v;
+        v.x = scale * ((bits & 1u ? 1.0f : -1.0f) + sigma * nrm[0]);
+        v.y = scale * ((bits & 2u ? 1.0f : -1.0f) + sigma * nrm[1]);
+        v.z = scale * ((bits & 4u ? 1.0f : -1.0f) + sigma * nrm[2]);
+        v.w = scale * ((bits & 8u ? 1.0f : -1.0f) + sigma * nrm[3]);
+        l4[j >> 2] = v;
+    }
+}
+
+/* per-frame Eb/N0 (Philox stream 2) and the noise scale, in float */
+__device__ __forceinline__ void frame_noise(const CodeDesc& c, const FramegenArgs& a, uint64_t g, float& ebno,
+                                            float& sigma, float& scale)
+{
+    uint32_t eo[4];
+    philox_at(a.seed, g, 0u, 2u, eo);
+    ebno = __fadd_rn(a.ebno_lo, __fmul_rn(__fsub_rn(a.ebno_hi, a.ebno_lo), unif24(eo[0])));
+    const float rate = (float)c.k / (float)c.n;
+    const float ebno_lin = exp10f(ebno * 0.1f);
+    const float sigma2 = 1.0f / (2.0f * rate * ebno_lin);
+    sigma = sqrtf(sigma2);
+    scale = 2.0f / sigma2;
+}
+
 constexpr int kEncWarps = 8;
 
 __global__ void __launch_bounds__(32 * kEncWarps)
@@ -97,15 +143,8 @@ framegen_kernel(CodeDesc c, FramegenArgs a)
     __syncwarp();
     warp_encode_parity(c, s, lane);
 
-    /* per-frame Eb/N0 and noise scale, in float */
-    uint32_t eo[4];
-    philox_at(a.seed, g, 0u, 2u, eo);
-    const float ebno = __fadd_rn(a.ebno_lo, __fmul_rn(__fsub_rn(a.ebno_hi, a.ebno_lo), unif24(eo[0])));
-    const float rate = (float)c.k / (float)c.n;
-    const float ebno_lin = exp10f(ebno * 0.1f);
-    const float sigma2 = 1.0f / (2.0f * rate * ebno_lin);
-    const float sigma = sqrtf(sigma2);
-    const float scale = 2.0f / sigma2;
+    float ebno, sigma, scale;
+    frame_noise(c, a, g, ebno, sigma, scale);
     if (a.ebno_out && lane == 0) a.ebno_out[f] = ebno;
 
     if (a.info) {
@@ -126,35 +165,67 @@ framegen_kernel(CodeDesc c, FramegenArgs a)
                 x4[(c.k + b * c.z + r) >> 2] = parity_bytes4(s, c.nw, b, r);
     }
     if (a.llr) {
-        float4* l4 = reinterpret_cast<float4*>(a.llr + f * c.n);
-        for (int j = lane * 4; j < c.n; j += 128) {
-            uint32_t bits;
-            if (j < c.k) {
-                bits = s.U[j >> 5] >> (j & 31);
-            } else {
-                const int p = j - c.k, b = p / c.z, r = p - b * c.z;
-                bits = s.out[b * c.nw + (r >> 5)] >> (r & 31);
-            }
-            uint32_t o[4];
-            philox_at(a.seed, g, (uint32_t)(j >> 2), 1u, o);
-            float nrm[4];
+        const uint32_t* U = s.U;
+        const uint32_t* out = s.out;
+        emit_llr(c, a, f, g, scale, sigma, lane, [&](int j) -> uint32_t {
+            if (j < c.k) return U[j >> 5] >> (j & 31);
+            const int p = j - c.k, b = p / c.z, r = p - b * c.z;
+            return out[b * c.nw + (r >> 5)] >> (r & 31);
+        });
+    }
+}
+
+
+/* Random codewords from the null space of H (any rate, 3/4B included): with
+ * H in reduced row-echelon form, pivot column p_i of row i and free columns
+ * F, a codeword takes random free bits u (Philox stream 0) and
+ * c[p_i] = parity(A_i & u), A_i = row i restricted to F. Then the same AWGN /
+ * LLR model as framegen_kernel. One warp per frame. */
+__global__ void __launch_bounds__(32 * kEncWarps)
+framegen_nullspace_kernel(CodeDesc c, FramegenArgs a, NullspaceArgs ns)
+{
+    __shared__ uint32_t s_u[kEncWarps][kMaxN / 32 + 4];
+    __shared__ uint32_t s_cw[kEncWarps][kMaxN / 32 + 4];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long f = (long long)blockIdx.x * kEncWarps + warp;
+    if (f >= a.frames) return;
+    const uint64_t g = a.first_frame + (uint64_t)f;
+    uint32_t* U = s_u[warp];
+    uint32_t* C = s_cw[warp];
+    const int fw = (ns.nfree + 31) / 32;
+    for (int q = lane; q * 4 < fw; q += 32) {
+        uint32_t o[4];
+        philox_at(a.seed, g, (uint32_t)q, 0u, o);
 #pragma unroll
-            for (int p = 0; p < 2; p++) {
-                const float u1 = unif24(o[2 * p]), u2 = unif24(o[2 * p + 1]);
-                const float rad = sqrtf(-2.0f * logf(u1));
-                float sn, cs;
-                sincospif(2.0f * u2, &sn, &cs);
-                nrm[2 * p] = rad * cs;
-                nrm[2 * p + 1] = rad * sn;
-            }
-            float4 v;
-            v.x = scale * ((bits & 1u ? 1.0f : -1.0f) + sigma * nrm[0]);
-            v.y = scale * ((bits & 2u ? 1.0f : -1.0f) + sigma * nrm[1]);
-            v.z = scale * ((bits & 4u ? 1.0f : -1.0f) + sigma * nrm[2]);
-            v.w = scale * ((bits & 8u ? 1.0f : -1.0f) + sigma * nrm[3]);
-            l4[j >> 2] = v;
+        for (int t = 0; t < 4; t++)
+            if (4 * q + t < fw) U[4 * q + t] = o[t];
+    }
+    for (int q = lane; q < c.n / 32 + 1; q += 32) C[q] = 0u;
+    __syncwarp();
+    if (lane == 0 && (ns.nfree & 31)) U[fw - 1] &= (1u << (ns.nfree & 31)) - 1u;
+    __syncwarp();
+    /* free bits */
+    for (int j = lane; j < ns.nfree; j += 32)
+        if ((U[j >> 5] >> (j & 31)) & 1u) atomicOr(&C[ns.free_col[j] >> 5], 1u << (ns.free_col[j] & 31));
+    /* pivot bits */
+    for (int i = lane; i < ns.rank; i += 32) {
+        const uint32_t* Ai = ns.A + (size_t)i * ns.words;
+        uint32_t par = 0;
+        for (int q = 0; q < fw; q++) par ^= __popc(Ai[q] & U[q]);
+        if (par & 1u) atomicOr(&C[ns.pivot_col[i] >> 5], 1u << (ns.pivot_col[i] & 31));
+    }
+    __syncwarp();
+    float ebno, sigma, scale;
+    frame_noise(c, a, g, ebno, sigma, scale);
+    if (a.ebno_out && lane == 0) a.ebno_out[f] = ebno;
+    if (a.cw) {
+        uint32_t* x4 = reinterpret_cast<uint32_t*>(a.cw + f * c.n);
+        for (int j = lane * 4; j < c.n; j += 128) {
+            const uint32_t w = C[j >> 5] >> (j & 31);
+            x4[j >> 2] = (w & 1u) | ((w & 2u) << 7) | ((w & 4u) << 14) | ((w & 8u) << 21);
         }
     }
+    if (a.llr) emit_llr(c, a, f, g, scale, sigma, lane, [&](int j) -> uint32_t { return C[j >> 5] >> (j & 31); });
 }
 
 /* One thread per expanded check row; rows of a frame are contiguous in
@@ -191,6 +262,37 @@ __global__ void bits_to_llr_kernel(const int8_t* __restrict__ bits, float* __res
         llr[i] = (float)__dadd_rn(__dmul_rn((double)bits[i], 2.0), -1.0);
 }
 
+/* The reference BER_runner's info-bit stream (reference lib/BER_runner.cc:35-41,
+ * 124-146): an LFSR x^31 + x^28 + 1 from 0xdeadbeef, restarted every 115200
+ * bits, so the stream is periodic. g_lfsr_period holds one period packed 32
+ * bits per word (written once per device from the host); bit p of the stream
+ * is bit (p mod 115200) of the period. */
+constexpr int kLfsrPeriod = 115200;
+__device__ uint32_t g_lfsr_period[kLfsrPeriod / 32];
+
+__global__ void lfsr_bits_kernel(unsigned long long first_bit, long long nbits, uint8_t* __restrict__ out)
+{
+    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nbits;
+         j += (long long)gridDim.x * blockDim.x) {
+        const unsigned p = (unsigned)((first_bit + (unsigned long long)j) % kLfsrPeriod);
+        out[j] = (uint8_t)((g_lfsr_period[p >> 5] >> (p & 31)) & 1u);
+    }
+}
+
+cudaError_t upload_lfsr_period(const uint32_t* words)
+{
+    return cudaMemcpyToSymbol(g_lfsr_period, words, sizeof(uint32_t) * (kLfsrPeriod / 32));
+}
+
+cudaError_t launch_lfsr_bits(unsigned long long first_bit, long long nbits, uint8_t* out, cudaStream_t st)
+{
+    if (nbits <= 0) return cudaSuccess;
+    long long blocks = (nbits + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    lfsr_bits_kernel<<<(unsigned)blocks, 256, 0, st>>>(first_bit, nbits, out);
+    return cudaGetLastError();
+}
+
 /* ---------------------------------------------------------------- launchers */
 
 cudaError_t launch_encode_bytes(const CodeDesc& c, const uint8_t* info, uint8_t* cw, long long frames,
@@ -207,6 +309,15 @@ cudaError_t launch_framegen(const CodeDesc& c, const FramegenArgs& a, cudaStream
     if (a.frames <= 0) return cudaSuccess;
     const long long blocks = (a.frames + kEncWarps - 1) / kEncWarps;
     framegen_kernel<<<(unsigned)blocks, 32 * kEncWarps, 0, st>>>(c, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_framegen_nullspace(const CodeDesc& c, const FramegenArgs& a, const NullspaceArgs& ns,
+                                      cudaStream_t st)
+{
+    if (a.frames <= 0) return cudaSuccess;
+    const long long blocks = (a.frames + kEncWarps - 1) / kEncWarps;
+    framegen_nullspace_kernel<<<(unsigned)blocks, 32 * kEncWarps, 0, st>>>(c, a, ns);
     return cudaGetLastError();
 }
 

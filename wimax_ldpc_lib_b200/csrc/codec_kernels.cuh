@@ -23,12 +23,27 @@ struct FramegenArgs {
     float* ebno_out;        /* frames, or null */
 };
 
+/* null-space description of H for random codewords: A is rank x words
+ * (row i restricted to the free columns, packed), pivot_col[rank],
+ * free_col[nfree] (device pointers) */
+struct NullspaceArgs {
+    const uint32_t* A;
+    const unsigned short* pivot_col;
+    const unsigned short* free_col;
+    int rank, nfree, words;
+};
+
+cudaError_t launch_framegen_nullspace(const CodeDesc& c, const FramegenArgs& a, const NullspaceArgs& ns,
+                                      cudaStream_t st);
 cudaError_t launch_encode_bytes(const CodeDesc& c, const uint8_t* info, uint8_t* cw, long long frames,
                                 cudaStream_t st);
 cudaError_t launch_framegen(const CodeDesc& c, const FramegenArgs& a, cudaStream_t st);
 cudaError_t launch_syndrome(const CodeDesc& c, const int8_t* bits, uint32_t* out, long long frames,
                             int early_exit, cudaStream_t st);
 cudaError_t launch_bits_to_llr(const int8_t* bits, float* llr, long long count, cudaStream_t st);
+/* the reference BER_runner's periodic LFSR info-bit stream */
+cudaError_t upload_lfsr_period(const uint32_t* words);
+cudaError_t launch_lfsr_bits(unsigned long long first_bit, long long nbits, uint8_t* out, cudaStream_t st);
 
 /* TDMP decoder specialised on (rate, z, mode) */
 struct TdmpLaunch {

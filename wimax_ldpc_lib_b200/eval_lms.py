@@ -1,0 +1,110 @@
+"""Evaluates trained learned min-sum weights against the plain decoder and
+records where they ship.
+
+  python -m wimax_ldpc_lib_b200.eval_lms weights/lms_r0_z96_T8.json [--frames 1048576]
+
+For every Eb/N0 point (default 1.0 to 3.0 dB in 0.25 dB steps) it generates
+held-out frames on the device (a seed and frame counters disjoint from
+training), decodes the same frames with the learned decoder at its trained cap T and at
+the reference's cap 10 (iterations past T reuse the last trained weights),
+and with the plain normalized min-sum at caps T and 10, and records FER, info
+BER, mean iterations and kernel-only info Gbit/s (CUDA events). The learned
+weights ship at a point and cap when their frame errors on those frames are
+no more than the plain decoder's at the same cap and they need fewer
+iterations on average (plain min-sum stays the judge and the fallback). The
+table is written back into the weight file under "evaluation".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+
+import wimax_ldpc_lib_b200 as wl  # noqa: E402
+
+EVAL_SEED = 0xE7A1
+
+
+def evaluate(meta, frames=1 << 20, batch=1 << 18, points=None, log=print):
+    import torch
+    rate, z, T = meta["rate"], meta["z"], meta["iterations"]
+    info_ = wl.code_info(rate, z)
+    n, k = info_.n, info_.k
+    points = points or [1.0 + 0.25 * i for i in range(9)]
+    batch = min(batch, frames)
+    w = np.array(meta["weights"], np.float32)
+    decs = {"learned": wl.LearnedDecoder(rate, z, T, weights=w),
+            "learned10": wl.LearnedDecoder(rate, z, T, weights=w, cap=10),
+            f"plain{T}": wl.Decoder(rate, z, T), "plain10": wl.Decoder(rate, z, 10)}
+    llr = torch.empty((batch, n), dtype=torch.float32, device="cuda")
+    info = torch.empty((batch, k), dtype=torch.uint8, device="cuda")
+    hard = torch.empty((batch, n), dtype=torch.int8, device="cuda")
+    st = torch.empty(batch, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+    rows = []
+    for p_i, eb in enumerate(points):
+        acc = {name: {"frame_errors": 0, "bit_errors": 0, "iterations": 0.0, "ms": 0.0} for name in decs}
+        done = 0
+        while done < frames:
+            nb = min(batch, frames - done)
+            wl.framegen_device(rate, z, EVAL_SEED, (1 << 40) + p_i * (1 << 32) + done, nb, eb, eb,
+                               info=info[:nb], llr=llr[:nb], stream=stream)
+            for name, dec in decs.items():
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                dec.decode_device(llr[:nb], hard[:nb], None, st[:nb], stream=stream)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                err = hard[:nb, :k].view(torch.uint8) != info[:nb]
+                a = acc[name]
+                a["frame_errors"] += int(err.any(dim=1).sum().item())
+                a["bit_errors"] += int(err.sum().item())
+                a["iterations"] += float((st[:nb] & 0xFFFF).double().sum().item())
+                a["ms"] += e0.elapsed_time(e1)
+            done += nb
+        row = {"ebno_db": eb, "frames": frames}
+        for name, a in acc.items():
+            row[name] = {"fer": a["frame_errors"] / frames, "frame_errors": a["frame_errors"],
+                         "ber": a["bit_errors"] / (frames * k), "mean_iterations": a["iterations"] / frames,
+                         "info_gbps": frames * k / (a["ms"] * 1e-3) / 1e9}
+        L, L10, P8, P = row["learned"], row["learned10"], row[f"plain{T}"], row["plain10"]
+        row["ship_cap10"] = bool(L10["frame_errors"] <= P["frame_errors"] and
+                                 L10["mean_iterations"] < P["mean_iterations"])
+        row[f"ship_cap{T}"] = bool(L["frame_errors"] <= P8["frame_errors"] and
+                                   L["mean_iterations"] < P8["mean_iterations"])
+        rows.append(row)
+        log(f"{eb:5.2f} dB | learned{T} FER {L['fer']:.2e} it {L['mean_iterations']:.2f} {L['info_gbps']:.1f} Gb/s "
+            f"| plain{T} FER {P8['fer']:.2e} it {P8['mean_iterations']:.2f} | learned10 FER {L10['fer']:.2e} "
+            f"it {L10['mean_iterations']:.2f} {L10['info_gbps']:.1f} Gb/s | plain10 FER {P['fer']:.2e} "
+            f"it {P['mean_iterations']:.2f} {P['info_gbps']:.1f} Gb/s | ship@10 {row['ship_cap10']} "
+            f"ship@{T} {row[f'ship_cap{T}']}")
+    return rows
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("weights")
+    ap.add_argument("--frames", type=int, default=1 << 20)
+    ap.add_argument("--points", type=float, nargs="*", default=None)
+    args = ap.parse_args()
+    with open(args.weights) as f:
+        meta = json.load(f)
+    rows = evaluate(meta, args.frames, points=args.points)
+    import torch
+    meta["evaluation"] = {"seed": EVAL_SEED, "frames_per_point": args.frames, "device": torch.cuda.get_device_name(0),
+                          "rule": "ship at a cap where learned frame errors <= plain frame errors at that cap on "
+                                  "the same held-out frames and learned mean iterations < plain mean iterations",
+                          "points": rows}
+    with open(args.weights, "w") as f:
+        json.dump(meta, f)
+    print(f"evaluation written into {args.weights}")
+
+
+if __name__ == "__main__":
+    main()
