@@ -134,6 +134,15 @@ WLDPC_API int wldpc_decode_batch_device(wldpc_decoder* dec, const float* llr, in
 WLDPC_API int wldpc_decode_batch_host(wldpc_decoder* dec, float* rx_codewords, int8_t* decoded, uint32_t* num_errors,
                             int32_t* status, size_t frames);
 
+/* Batch form of decode(int8_t*, int8_t*) over host buffers (frames x n bytes
+ * in and out; num_errors nullable), as the reference's test_decoder drives it
+ * (reference lib/decode_example.cc:128-135). Synchronous. */
+WLDPC_API int wldpc_decode_bits_batch_host(wldpc_decoder* dec, const int8_t* bits, int8_t* decoded,
+                                           uint32_t* num_errors, size_t frames);
+/* Batch form of compute_syndrome(int8_t*, bool) over host buffers. */
+WLDPC_API int wldpc_syndrome_batch_host(wldpc_decoder* dec, const int8_t* bits, int exit_early, uint32_t* counts,
+                                        size_t frames);
+
 /* Waits for the device and reports a device-side error (WLDPC_ERR_TIMEOUT)
  * recorded by earlier launches of this decoder. */
 WLDPC_API int wldpc_decoder_synchronize(wldpc_decoder* dec);
@@ -153,6 +162,9 @@ WLDPC_API int wldpc_encoder_destroy(wldpc_encoder* enc);
  * (reference include/ldpc_encoder.h:24, lib/ldpc_encoder.cc:50-105): k input
  * bytes (non-zero = 1), n output bytes, systematic part copied verbatim. */
 WLDPC_API int wldpc_encoder_encode(wldpc_encoder* enc, const uint8_t* infoword, uint8_t* codeword);
+
+/* Batched encode of host buffers (frames x k in, frames x n out). Synchronous. */
+WLDPC_API int wldpc_encode_batch_host(wldpc_encoder* enc, const uint8_t* info, uint8_t* codeword, size_t frames);
 
 /* Batched encode on device memory (frames x k in, frames x n out, both
  * 4-byte aligned), asynchronous on stream (NULL = the CUDA default stream). */
@@ -184,8 +196,8 @@ WLDPC_API int wldpc_framegen_device(int rate, unsigned z, uint64_t seed, uint64_
  * trained on the GPU by the library's own forward/backward kernels and Adam.
  * Weight tables are float[2][T][12][24]: a then b, [iteration][layer][column];
  * entries of all-zero blocks are ignored (returned as 0). Supported codes:
- * every rate at z = 24, 48, 96 (WLDPC_ERR_UNSUPPORTED otherwise); training
- * needs an encoder, so not rate 3/4B. A new handle starts at a = 0.815, b = 0. */
+ * every rate at z = 24, 48, 96 (WLDPC_ERR_UNSUPPORTED otherwise); 3/4B
+ * trains on null-space codewords. A new handle starts at a = 0.815, b = 0. */
 typedef struct wldpc_lms wldpc_lms;
 WLDPC_API int wldpc_lms_create(int rate, unsigned z, unsigned iterations, wldpc_lms** out);
 WLDPC_API int wldpc_lms_destroy(wldpc_lms* h);
@@ -206,7 +218,8 @@ WLDPC_API int wldpc_lms_decode_host(wldpc_lms* h, float* rx_codewords, int8_t* d
 WLDPC_API int wldpc_lms_loss_grad(wldpc_lms* h, const float* llr, const uint8_t* codeword, size_t frames,
                                   float* grad_table, double* loss);
 /* `steps` Adam steps (lr, beta 0.9 / 0.999) on batches of `batch` frames
- * generated on the device (wldpc_framegen_device, Eb/N0 uniform in
+ * generated on the device (wldpc_framegen_device, or
+ * wldpc_framegen_nullspace_device for 3/4B; Eb/N0 uniform in
  * [ebno_lo_db, ebno_hi_db], frame counter first_frame + step * batch).
  * loss_history (nullable) receives the batch loss of every step. */
 WLDPC_API int wldpc_lms_train(wldpc_lms* h, unsigned steps, unsigned batch, float ebno_lo_db, float ebno_hi_db,

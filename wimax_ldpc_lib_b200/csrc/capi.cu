@@ -320,6 +320,47 @@ int wldpc_decoder_compute_syndrome(wldpc_decoder* d, const int8_t* rx_codeword, 
     return WLDPC_OK;
 }
 
+/* Batched forms of decode(int8_t*) and compute_syndrome over host buffers. */
+int wldpc_decode_bits_batch_host(wldpc_decoder* d, const int8_t* bits, int8_t* decoded, uint32_t* num_errors,
+                                 size_t frames)
+{
+    if (!d || (frames && (!bits || !decoded))) return WLDPC_ERR_ARG;
+    if (frames == 0) return WLDPC_OK;
+    const size_t n = (size_t)d->code.n;
+    int rc;
+    if ((rc = d->bits.reserve(frames * n)) || (rc = d->llr.reserve(frames * n * 4)) ||
+        (rc = d->hard.reserve(frames * n)) || (rc = d->status.reserve(frames * 4)))
+        return rc;
+    CU(cudaMemcpyAsync(d->bits.p, bits, frames * n, cudaMemcpyHostToDevice, d->stream));
+    CU(launch_bits_to_llr((const int8_t*)d->bits.p, (float*)d->llr.p, (long long)(frames * n), d->stream));
+    if ((rc = decode_launch(d, (const float*)d->llr.p, (int8_t*)d->hard.p, nullptr, (int32_t*)d->status.p, frames,
+                            d->stream)))
+        return rc;
+    std::vector<int32_t> st(frames);
+    CU(cudaMemcpyAsync(decoded, d->hard.p, frames * n, cudaMemcpyDeviceToHost, d->stream));
+    CU(cudaMemcpyAsync(st.data(), d->status.p, frames * 4, cudaMemcpyDeviceToHost, d->stream));
+    CU(cudaStreamSynchronize(d->stream));
+    if ((rc = read_err(d))) return rc;
+    if (num_errors)
+        for (size_t f = 0; f < frames; f++) num_errors[f] = ref_return(d, st[f]);
+    return WLDPC_OK;
+}
+
+int wldpc_syndrome_batch_host(wldpc_decoder* d, const int8_t* bits, int exit_early, uint32_t* counts, size_t frames)
+{
+    if (!d || (frames && (!bits || !counts))) return WLDPC_ERR_ARG;
+    if (frames == 0) return WLDPC_OK;
+    const size_t n = (size_t)d->code.n;
+    int rc;
+    if ((rc = d->bits.reserve(frames * n)) || (rc = d->status.reserve(frames * 4))) return rc;
+    CU(cudaMemcpyAsync(d->bits.p, bits, frames * n, cudaMemcpyHostToDevice, d->stream));
+    CU(launch_syndrome(d->code, (const int8_t*)d->bits.p, (uint32_t*)d->status.p, (long long)frames, exit_early,
+                       d->stream));
+    CU(cudaMemcpyAsync(counts, d->status.p, frames * 4, cudaMemcpyDeviceToHost, d->stream));
+    CU(cudaStreamSynchronize(d->stream));
+    return WLDPC_OK;
+}
+
 /* Host batch: chunks alternate between two streams so that the copy-in of
  * one chunk, the kernel of another and the copy-out of a third overlap. */
 int wldpc_decode_batch_host(wldpc_decoder* d, float* rx, int8_t* decoded, uint32_t* num_errors,
@@ -395,6 +436,19 @@ int wldpc_encoder_destroy(wldpc_encoder* e)
         cudaStreamDestroy(e->stream);
     }
     delete e;
+    return WLDPC_OK;
+}
+
+int wldpc_encode_batch_host(wldpc_encoder* e, const uint8_t* info, uint8_t* codeword, size_t frames)
+{
+    if (!e || (frames && (!info || !codeword))) return WLDPC_ERR_ARG;
+    if (frames == 0) return WLDPC_OK;
+    int rc;
+    if ((rc = e->info.reserve(frames * e->code.k)) || (rc = e->cw.reserve(frames * e->code.n))) return rc;
+    CU(cudaMemcpyAsync(e->info.p, info, frames * e->code.k, cudaMemcpyHostToDevice, e->stream));
+    CU(launch_encode_bytes(e->code, (const uint8_t*)e->info.p, (uint8_t*)e->cw.p, (long long)frames, e->stream));
+    CU(cudaMemcpyAsync(codeword, e->cw.p, frames * e->code.n, cudaMemcpyDeviceToHost, e->stream));
+    CU(cudaStreamSynchronize(e->stream));
     return WLDPC_OK;
 }
 
@@ -524,6 +578,23 @@ int nullspace_for(int rate, int z, Nullspace** out)
 }
 
 }  // namespace
+
+/* null-space frame generation for other parts of the library (learned
+ * training); internal, C linkage because it sits in this file's extern "C" block */
+int wldpc_internal_nullspace_frames(int rate, int z, const FramegenArgs& a, cudaStream_t st)
+{
+    Nullspace* ns = nullptr;
+    int rc = nullspace_for(rate, z, &ns);
+    if (rc) return rc;
+    NullspaceArgs na;
+    na.A = (const uint32_t*)ns->A.p;
+    na.pivot_col = (const unsigned short*)ns->piv.p;
+    na.free_col = (const unsigned short*)ns->fre.p;
+    na.rank = ns->rank;
+    na.nfree = ns->nfree;
+    na.words = ns->words;
+    return launch_framegen_nullspace(make_code_desc(rate, z), a, na, st) == cudaSuccess ? WLDPC_OK : WLDPC_ERR_CUDA;
+}
 
 int wldpc_framegen_nullspace_device(int rate, unsigned z, uint64_t seed, uint64_t first_frame, size_t frames,
                                     float ebno_lo_db, float ebno_hi_db, uint8_t* codeword, float* llr, float* ebno_db,

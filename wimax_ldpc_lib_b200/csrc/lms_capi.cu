@@ -18,6 +18,8 @@
 
 using namespace wldpc;
 
+extern "C" int wldpc_internal_nullspace_frames(int rate, int z, const wldpc::FramegenArgs& a, cudaStream_t st);
+
 namespace wldpc {
 extern const LmsLaunch kLms_r0[kLmsNumZ];
 extern const LmsLaunch kLms_r1[kLmsNumZ];
@@ -418,7 +420,6 @@ int wldpc_lms_train(wldpc_lms* h, unsigned steps, unsigned batch, float ebno_lo_
                     uint64_t first_frame, float lr, float* loss_history)
 {
     if (!h || batch == 0) return WLDPC_ERR_ARG;
-    if (h->rate == THREEQUARTERSB) return WLDPC_ERR_UNSUPPORTED;   /* no encoder for frame generation */
     if (h->host_stale == false) {
         int rc = lms_push_device_weights(h);
         if (rc) return rc;
@@ -437,7 +438,11 @@ int wldpc_lms_train(wldpc_lms* h, unsigned steps, unsigned batch, float ebno_lo_
         f.ebno_hi = ebno_hi_db;
         f.cw = (uint8_t*)h->tcw.p;
         f.llr = (float*)h->tllr.p;
-        CU(launch_framegen(h->code, f, h->stream));
+        if (h->rate == THREEQUARTERSB) {   /* no dual-diagonal encoder: null-space codewords */
+            if ((rc = wldpc_internal_nullspace_frames(h->rate, h->z, f, h->stream))) return rc;
+        } else {
+            CU(launch_framegen(h->code, f, h->stream));
+        }
         if ((rc = lms_forward_backward(h, (const float*)h->tllr.p, (const uint8_t*)h->tcw.p, batch, h->stream)))
             return rc;
         if ((rc = lms_reduce(h, batch, 1, lr, (float*)h->loss.p + s, h->stream))) return rc;

@@ -327,6 +327,7 @@ struct wldpc_mixed {
     unsigned max_iter;
     int threads = 96, chunk = 32;
     int sms = 148;
+    int per_sm[2][kRates] = {};   /* resident CTAs per SM, [96 | 192 threads][rate] */
     cudaStream_t stream = nullptr;
     cudaStream_t rs[kRates] = {};
     cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_fork = nullptr, ev_join[kRates] = {};
@@ -344,6 +345,9 @@ struct wldpc_mixed {
 };
 
 using MixedKernel = void (*)(const MixedArgs);
+/* dynamic shared memory of a CTA: posteriors (24 floats per thread) and the
+ * 16-bit address table (96 blocks per thread) */
+static int mixed_smem(int threads) { return 24 * threads * 4 + 96 * threads * 2; }
 template <int T>
 struct MixedKernels {
     static constexpr MixedKernel k[kRates] = {&mixed_decode_kernel<0, T>, &mixed_decode_kernel<1, T>,
@@ -380,21 +384,29 @@ static int mixed_enqueue(wldpc_mixed* h, const uint8_t* variant, const long long
     a.frames = nf;
     a.max_iter = (int)h->max_iter;
     const int T = h->threads;
-    const int smem = 24 * T * 4 + 96 * T * 2;
+    const int ti = T == 96 ? 0 : 1;
+    const int smem = mixed_smem(T);
     /* fork: the six rate kernels run concurrently, then join back on st */
-    if (cudaEventRecord(h->ev_fork, st) != cudaSuccess) return WLDPC_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess || cudaEventRecord(h->ev_fork, st) != cudaSuccess) return WLDPC_ERR_CUDA;
+    /* every forked stream is joined back even when a step fails, so that a
+     * capture in progress always ends with all its streams joined */
+    int rc = WLDPC_OK;
     for (int rate = 0; rate < kRates; rate++) {
-        const MixedKernel k = T == 96 ? MixedKernels<96>::k[rate] : MixedKernels<192>::k[rate];
-        int per_sm = 1;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, T, smem);
-        if (cudaStreamWaitEvent(h->rs[rate], h->ev_fork, 0) != cudaSuccess) return WLDPC_ERR_CUDA;
-        k<<<h->sms * (per_sm > 0 ? per_sm : 1), T, smem, h->rs[rate]>>>(a);
-        if (cudaGetLastError() != cudaSuccess) return WLDPC_ERR_CUDA;
+        const MixedKernel k = ti == 0 ? MixedKernels<96>::k[rate] : MixedKernels<192>::k[rate];
+        const int per_sm = h->per_sm[ti][rate];
+        if (cudaStreamWaitEvent(h->rs[rate], h->ev_fork, 0) != cudaSuccess) {
+            rc = WLDPC_ERR_CUDA;
+            break;
+        }
+        k<<<h->sms * per_sm, T, smem, h->rs[rate]>>>(a);
+        if (cudaGetLastError() != cudaSuccess) rc = WLDPC_ERR_CUDA;
         if (cudaEventRecord(h->ev_join[rate], h->rs[rate]) != cudaSuccess ||
-            cudaStreamWaitEvent(st, h->ev_join[rate], 0) != cudaSuccess)
-            return WLDPC_ERR_CUDA;
+            cudaStreamWaitEvent(st, h->ev_join[rate], 0) != cudaSuccess) {
+            rc = WLDPC_ERR_CUDA;
+            break;
+        }
     }
-    return WLDPC_OK;
+    return rc;
 }
 
 extern "C" {
@@ -423,6 +435,20 @@ int wldpc_mixed_create(unsigned max_iter, wldpc_mixed** out)
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev);
+    /* shared-memory limit and occupancy of every decode kernel, once, outside any capture */
+    for (int ti = 0; ti < 2; ti++)
+        for (int rate = 0; rate < kRates; rate++) {
+            const int T = ti == 0 ? 96 : 192;
+            const MixedKernel k = ti == 0 ? MixedKernels<96>::k[rate] : MixedKernels<192>::k[rate];
+            int per = 0;
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, mixed_smem(T)) != cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, T, mixed_smem(T)) != cudaSuccess) {
+                cudaGetLastError();
+                delete h;
+                return WLDPC_ERR_CUDA;
+            }
+            h->per_sm[ti][rate] = per > 0 ? per : 1;
+        }
     bool ok = true;
     for (int r = 0; r < kRates; r++)
         ok = ok && cudaStreamCreateWithFlags(&h->rs[r], cudaStreamNonBlocking) == cudaSuccess &&
@@ -489,8 +515,6 @@ int wldpc_mixed_decode_device(wldpc_mixed* h, const uint8_t* variant, const int6
     if ((rc = h->rank.reserve(frames * sizeof(int))) || (rc = h->perm.reserve(frames * sizeof(int))) ||
         (rc = h->items.reserve(max_items * sizeof(MixedItem))))
         return rc;
-    const int smem = 24 * h->threads * 4;
-    (void)smem;
     wldpc_mixed::Key key{variant, offset, llr, decoded, posterior, status, frames, h->threads, h->chunk};
     const cudaStream_t user = (cudaStream_t)stream;
     if (cudaEventRecord(h->ev_in, user) != cudaSuccess || cudaStreamWaitEvent(h->stream, h->ev_in, 0) != cudaSuccess) {
@@ -566,14 +590,18 @@ int wldpc_mixed_autotune(wldpc_mixed* h, const uint8_t* variant, const int64_t* 
             h->threads = kThreadChoices[ti];
             h->chunk = chunks[ci];
             int rc = wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr, frames, h->stream);
-            if (rc) return rc;
-            cudaEventRecord(e0, h->stream);
-            for (int k = 0; k < repeats; k++)
-                wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr, frames, h->stream);
-            cudaEventRecord(e1, h->stream);
-            if (cudaEventSynchronize(e1) != cudaSuccess) {
+            if (!rc && cudaEventRecord(e0, h->stream) != cudaSuccess) rc = WLDPC_ERR_CUDA;
+            for (int k = 0; k < repeats && !rc; k++)
+                rc = wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr, frames, h->stream);
+            if (!rc && (cudaEventRecord(e1, h->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
+                rc = WLDPC_ERR_CUDA;
+            if (rc) {
                 cudaGetLastError();
-                return WLDPC_ERR_CUDA;
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                h->threads = bt;
+                h->chunk = bc;
+                return rc;
             }
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);

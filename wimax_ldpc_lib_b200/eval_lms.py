@@ -36,14 +36,17 @@ def evaluate(meta, frames=1 << 20, batch=1 << 18, points=None, log=print):
     rate, z, T = meta["rate"], meta["z"], meta["iterations"]
     info_ = wl.code_info(rate, z)
     n, k = info_.n, info_.k
-    points = points or [1.0 + 0.25 * i for i in range(9)]
+    lo = meta.get("training", {}).get("ebno_db", [1.0, 3.0])[0]
+    points = points or [lo + 0.25 * i for i in range(9)]
     batch = min(batch, frames)
+    # 3/4B has no encoder: frames are null-space codewords and errors count over all n bits
+    kk = n if rate == 4 else k
     w = np.array(meta["weights"], np.float32)
     decs = {"learned": wl.LearnedDecoder(rate, z, T, weights=w),
             "learned10": wl.LearnedDecoder(rate, z, T, weights=w, cap=10),
             f"plain{T}": wl.Decoder(rate, z, T), "plain10": wl.Decoder(rate, z, 10)}
     llr = torch.empty((batch, n), dtype=torch.float32, device="cuda")
-    info = torch.empty((batch, k), dtype=torch.uint8, device="cuda")
+    info = torch.empty((batch, kk), dtype=torch.uint8, device="cuda")
     hard = torch.empty((batch, n), dtype=torch.int8, device="cuda")
     st = torch.empty(batch, dtype=torch.int32, device="cuda")
     stream = torch.cuda.Stream()
@@ -53,15 +56,19 @@ def evaluate(meta, frames=1 << 20, batch=1 << 18, points=None, log=print):
         done = 0
         while done < frames:
             nb = min(batch, frames - done)
-            wl.framegen_device(rate, z, EVAL_SEED, (1 << 40) + p_i * (1 << 32) + done, nb, eb, eb,
-                               info=info[:nb], llr=llr[:nb], stream=stream)
+            first = (1 << 40) + p_i * (1 << 32) + done
+            if rate == 4:
+                wl.framegen_nullspace_device(rate, z, EVAL_SEED, first, nb, eb, eb, codeword=info[:nb], llr=llr[:nb],
+                                             stream=stream)
+            else:
+                wl.framegen_device(rate, z, EVAL_SEED, first, nb, eb, eb, info=info[:nb], llr=llr[:nb], stream=stream)
             for name, dec in decs.items():
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
                 dec.decode_device(llr[:nb], hard[:nb], None, st[:nb], stream=stream)
                 e1.record(stream)
                 torch.cuda.synchronize()
-                err = hard[:nb, :k].view(torch.uint8) != info[:nb]
+                err = hard[:nb, :kk].view(torch.uint8) != info[:nb]
                 a = acc[name]
                 a["frame_errors"] += int(err.any(dim=1).sum().item())
                 a["bit_errors"] += int(err.sum().item())
@@ -71,7 +78,7 @@ def evaluate(meta, frames=1 << 20, batch=1 << 18, points=None, log=print):
         row = {"ebno_db": eb, "frames": frames}
         for name, a in acc.items():
             row[name] = {"fer": a["frame_errors"] / frames, "frame_errors": a["frame_errors"],
-                         "ber": a["bit_errors"] / (frames * k), "mean_iterations": a["iterations"] / frames,
+                         "ber": a["bit_errors"] / (frames * kk), "mean_iterations": a["iterations"] / frames,
                          "info_gbps": frames * k / (a["ms"] * 1e-3) / 1e9}
         L, L10, P8, P = row["learned"], row["learned10"], row[f"plain{T}"], row["plain10"]
         row["ship_cap10"] = bool(L10["frame_errors"] <= P["frame_errors"] and
