@@ -31,6 +31,41 @@ __device__ __forceinline__ void static_for(F&& f)
     static_for_impl(f, std::make_integer_sequence<int, N>{});
 }
 
+/* m1 <= m2: the two smallest of |v[LO]| .. |v[HI-1]|, counted with
+ * multiplicity (two equal minima give m1 == m2), by a balanced tree of
+ * fminf/fmaxf. For non-NaN inputs the values equal those of the sequential
+ * scan m2 = min(m2, max(m1, |v|)), m1 = min(m1, |v|), with a dependency depth
+ * of log2(HI - LO) instead of HI - LO. */
+template <int LO, int HI, int D>
+__device__ __forceinline__ void two_min_abs(const float (&v)[D], float& m1, float& m2)
+{
+    static_assert(HI - LO >= 2, "two_min_abs needs two values");
+    if constexpr (HI - LO == 2) {
+        m1 = fminf(fabsf(v[LO]), fabsf(v[LO + 1]));
+        m2 = fmaxf(fabsf(v[LO]), fabsf(v[LO + 1]));
+    } else if constexpr (HI - LO == 3) {
+        float a1, a2;
+        two_min_abs<LO, LO + 2>(v, a1, a2);
+        const float c = fabsf(v[LO + 2]);
+        m1 = fminf(a1, c);
+        m2 = fminf(fmaxf(a1, c), a2);
+    } else {
+        constexpr int H = HI - LO;
+        constexpr int MID = LO + (H >= 16 ? 8 * (H / 16) : H >= 8 ? 4 * (H / 8) : 2 * (H / 4));
+        float a1, a2, b1, b2;
+        two_min_abs<LO, MID>(v, a1, a2);
+        if constexpr (HI - MID == 1) {
+            const float c = fabsf(v[MID]);
+            m1 = fminf(a1, c);
+            m2 = fminf(fmaxf(a1, c), a2);
+        } else {
+            two_min_abs<MID, HI>(v, b1, b2);
+            m1 = fminf(a1, b1);
+            m2 = fminf(fmaxf(a1, b1), fminf(a2, b2));
+        }
+    }
+}
+
 __device__ __forceinline__ uint32_t smem_addr(const void* p)
 {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));

@@ -19,10 +19,12 @@
  * the reference's stopping rule (slice x >= 0, stop at a zero syndrome).
  * Weights a = 0.815, b = 0 give a float normalized min-sum.
  *
- * Messages: the decoder keeps every edge's message in shared memory
- * (block-major, [block][row]), so pass 1 reads the old message with one
- * load instead of recomputing it from compressed state and the weights of
- * the previous iteration. All arithmetic is fp32.
+ * Messages: the decoder keeps every edge's message in a register of the
+ * thread that owns the edge's row (one per non-zero block: 76 to 88), so
+ * pass 1 reads the old message without a load and without recomputing it
+ * from compressed state and the previous iteration's weights; shared memory
+ * holds only the posteriors and the weights (as (a, b) pairs, one 8-byte
+ * broadcast load per edge). All arithmetic is fp32.
  *
  * Training (one frame per CTA of z threads): the forward pass runs all T
  * iterations, stores the posterior and the messages at every iteration
@@ -77,9 +79,11 @@ struct LmsShape {
     static constexpr int E = NBLK * Z;
     /* frames per CTA: whole warps when that fits in ~100 KB, else one */
     static constexpr int GW = 32 / gcd_c(Z, 32);
-    static constexpr int G = GW * (N + E) * 4 <= 100 * 1024 ? GW : 1;
+    static constexpr int G = GW * N * 4 <= 100 * 1024 ? GW : 1;
     static constexpr int THREADS = G * Z;
-    static constexpr int SMEM = G * (N + E) * 4;
+    /* posteriors of G frames, then the weights as (a, b) pairs */
+    static constexpr int WOFF = G * N;
+    static constexpr int SMEM = WOFF * 4 + kLmsMaxIter * NBLK * 8;
 };
 
 /* ------------------------------------------------------------ inference */
@@ -89,7 +93,7 @@ __global__ void __launch_bounds__(LmsShape<R, Z>::THREADS)
 lms_decode_kernel(const __grid_constant__ LmsArgs a)
 {
     using S = LmsShape<R, Z>;
-    constexpr int MB = S::MB, N = S::N, E = S::E, G = S::G;
+    constexpr int MB = S::MB, N = S::N, G = S::G;
     extern __shared__ __align__(128) float smem_lms[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ unsigned s_fail[2];
@@ -101,7 +105,9 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
     const long long left = a.frames - f0;
     const int nf = left < G ? (int)left : G;
     float* P = smem_lms + g * N;                 /* posteriors of frame g */
-    float* M = smem_lms + G * N + g * E;         /* messages of frame g, [block][row] */
+    float* const Pr = P + r;
+    float* const Prz = Pr - Z;
+    float2* sw = reinterpret_cast<float2*>(smem_lms + S::WOFF);   /* [iteration][block] (a, b) */
 
     if (tid == 0) {
         mbar_init(&bar, 1);
@@ -112,7 +118,10 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         mbar_arrive_expect_tx(&bar, bytes);
         bulk_g2s(smem_lms, a.llr + f0 * N, bytes, &bar);
     }
-    for (int q = tid; q < G * E; q += S::THREADS) smem_lms[G * N + q] = 0.0f;
+    for (int q = tid; q < a.wrows * S::NBLK; q += S::THREADS) {
+        const int t = q / S::NBLK, b = q - t * S::NBLK;
+        sw[q] = make_float2(a.w.a[t][b], a.w.b[t][b]);
+    }
     __syncthreads();
     const bool ok = mbar_wait_bounded(&bar, 0);
     if (__syncthreads_or(!ok)) {
@@ -127,11 +136,11 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         unsigned fail = 0;
         static_for<MB>([&](auto I) {
             constexpr int d = layer_degree(R, I);
-            uint32_t acc = (uint32_t)(d & 1) << 31;
+            bool odd = (d & 1) != 0;   /* parity of the hard bits: d minus the negatives */
             static_for<d>([&](auto E_) {
-                acc ^= __float_as_uint(canon(P[edge_var_c<R, Z, I, E_>(r)]));
+                odd = odd != (*edge_ptr<R, Z, I, E_>(Pr, Prz, r) < 0.0f);
             });
-            fail |= acc >> 31;
+            fail |= odd ? 1u : 0u;
         });
         return fail;
     };
@@ -144,6 +153,12 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
             return s_fail[slot];
         }
     };
+
+    /* this thread's check-to-variable messages, one per block (its row of every
+     * layer), in registers: every index is a compile-time constant */
+    float Mr[S::NBLK];
+#pragma unroll
+    for (int q = 0; q < S::NBLK; q++) Mr[q] = 0.0f;
 
     const bool live = g < nf;
     unsigned fmask = frame_fail(live ? rows_fail() : 0u, 0);
@@ -159,32 +174,29 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
             constexpr int b0 = block_index(R, I, 0);
             if (active) {
                 float L[d];
-                uint32_t sgn = 0;
-                float m1 = __int_as_float(0x7f800000), m2 = __int_as_float(0x7f800000);
+                uint32_t par = 0;   /* bit 31: parity of the negative L */
                 static_for<d>([&](auto E_) {
                     constexpr int e = decltype(E_)::value;
-                    const float x = P[edge_var_c<R, Z, I, e>(r)];
-                    const float l = __fsub_rn(x, M[(b0 + e) * Z + r]);
+                    const float x = *edge_ptr<R, Z, I, e>(Pr, Prz, r);
+                    const float l = __fsub_rn(x, Mr[b0 + e]);
                     L[e] = l;
-                    sgn = __funnelshift_l(__float_as_uint(l), sgn, 1);
-                    const float al = fabsf(l);
-                    m2 = fminf(m2, fmaxf(m1, al));
-                    m1 = fminf(m1, al);
+                    par ^= __float_as_uint(l);
                 });
+                float m1, m2;
+                two_min_abs<0, d>(L, m1, m2);
                 /* positive LLR = bit 1: the extrinsic sign flips on odd-degree rows */
-                const uint32_t fb = (uint32_t)((__popc(sgn) & 1) ^ (d & 1)) << 31;
-                const int wr = t < a.wrows ? t : a.wrows - 1;
-                const float* wa = a.w.a[wr];
-                const float* wb = a.w.b[wr];
+                const uint32_t fb = (par ^ ((uint32_t)(d & 1) << 31)) & 0x80000000u;
+                const float2* wt = sw + (t < a.wrows ? t : a.wrows - 1) * S::NBLK;
                 static_for<d>([&](auto E_) {
                     constexpr int e = decltype(E_)::value;
                     const float l = L[e];
                     const float mu = (fabsf(l) == m1) ? m2 : m1;
-                    const float mag = fmaxf(__fmaf_rn(wa[b0 + e], mu, -wb[b0 + e]), 0.0f);
+                    const float2 ab = wt[b0 + e];
+                    const float mag = fmaxf(__fmaf_rn(ab.x, mu, -ab.y), 0.0f);
                     const uint32_t sb = (__float_as_uint(l) ^ fb) & 0x80000000u;
                     const float msg = __uint_as_float(__float_as_uint(mag) | sb);
-                    M[(b0 + e) * Z + r] = msg;
-                    P[edge_var_c<R, Z, I, e>(r)] = __fadd_rn(l, msg);
+                    Mr[b0 + e] = msg;
+                    *edge_ptr<R, Z, I, e>(Pr, Prz, r) = __fadd_rn(l, msg);
                 });
             }
             __syncthreads();

@@ -92,11 +92,11 @@ __device__ __forceinline__ void mixed_run_item(const MixedArgs& a, const MixedIt
             unsigned fail = 0;
             static_for<MB>([&](auto I) {
                 constexpr int d = layer_degree(R, I);
-                uint32_t acc = (uint32_t)(d & 1) << 31;
+                bool odd = (d & 1) != 0;   /* parity of the hard bits: d minus the negatives */
                 static_for<d>([&](auto E_) {
-                    acc ^= __float_as_uint(canon(P[mixed_var<R, I, E_, THREADS>(A)]));
+                    odd = odd != (P[mixed_var<R, I, E_, THREADS>(A)] < 0.0f);
                 });
-                fail |= acc >> 31;
+                fail |= odd ? 1u : 0u;
             });
             if (fail) atomicOr(&S.fail, 1u << g);
         }
@@ -136,7 +136,7 @@ __device__ __forceinline__ void mixed_run_item(const MixedArgs& a, const MixedIt
                 float L[d];
                 uint32_t LC[d];
                 uint32_t sgn = 0;
-                float m1 = 10000.0f, m2 = 10000.0f;
+                float m1, m2;
                 const float oM1 = M1[I], oM2 = M2[I];
                 const uint32_t oNeg = NEG[I];
                 const int oIdx = (int)(oNeg >> 27);
@@ -149,10 +149,11 @@ __device__ __forceinline__ void mixed_run_item(const MixedArgs& a, const MixedIt
                     L[e] = l;
                     LC[e] = __float_as_uint(canon(l));
                     sgn = __funnelshift_l(LC[e], sgn, 1);
-                    const float al = fabsf(l);
-                    m2 = fminf(m2, fmaxf(m1, al));
-                    m1 = fminf(m1, al);
                 });
+                /* the two smallest |L| from 10000.0f (reference lib/ldpc_decoder.cc:150,198) */
+                two_min_abs<0, d>(L, m1, m2);
+                m1 = fminf(m1, 10000.0f);
+                m2 = fminf(m2, 10000.0f);
                 const uint32_t flip = (uint32_t)((d & 1) ^ (__popc(sgn) & 1));
                 const uint32_t dmask = (d >= 32) ? 0xffffffffu : ((1u << d) - 1u);
                 const double D1 = __dmul_rn((double)m1, 0.815);

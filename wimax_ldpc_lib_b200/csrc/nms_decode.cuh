@@ -93,6 +93,23 @@ __device__ __forceinline__ int edge_var_c(int r)
     return col * Z + t;
 }
 
+/* posterior of edge E of layer I for row r, z a compile-time constant, given
+ * Pr = P + r and Prz = P + r - Z: the row's variable is col*Z + (r + s) mod Z,
+ * i.e. Pr or Prz (whichever keeps r + s - {0, Z} inside the block) plus the
+ * constant col*Z + s, so an edge costs one compare and one select and the
+ * constant folds into the shared-memory access */
+template <int R, int Z, int I, int E>
+__device__ __forceinline__ float* edge_ptr(float* Pr, float* Prz, int r)
+{
+    constexpr int col = layer_col(R, I, E);
+    constexpr int s = layer_shift(R, Z, I, E);
+    if constexpr (s == 0) {
+        return Pr + col * Z;
+    } else {
+        return ((r < Z - s) ? Pr : Prz) + (col * Z + s);
+    }
+}
+
 /* variable index of edge E of layer I for row r */
 template <int R, int ZT, int I, int E>
 __device__ __forceinline__ int edge_var(int r, const DecodeArgs& a)
@@ -104,6 +121,18 @@ __device__ __forceinline__ int edge_var(int r, const DecodeArgs& a)
         int t = r + (int)a.shift[b];
         t = (t >= a.z) ? t - a.z : t;
         return (int)a.colz[b] + t;
+    }
+}
+
+/* posterior of edge E of layer I for row r: edge_ptr when z is a
+ * compile-time constant, else the run-time-z index */
+template <int R, int ZT, int I, int E>
+__device__ __forceinline__ float* post_ptr(float* P, float* Pr, float* Prz, int r, const DecodeArgs& a)
+{
+    if constexpr (ZT > 0) {
+        return edge_ptr<R, ZT, I, E>(Pr, Prz, r);
+    } else {
+        return P + edge_var<R, ZT, I, E>(r, a);
     }
 }
 
@@ -129,6 +158,8 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
     const long long left = a.frames - f0;
     const int nf = left < G ? (int)left : G;
     float* P = smem_post + g * N;
+    float* const Pr = P + r;
+    float* const Prz = Pr - Z;
 
     if (tid == 0) {
         mbar_init(&bar, 1);
@@ -154,11 +185,11 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
         unsigned fail = 0;
         static_for<MB>([&](auto I) {
             constexpr int d = layer_degree(R, I);
-            uint32_t acc = (uint32_t)(d & 1) << 31;
+            bool odd = (d & 1) != 0;   /* parity of the hard bits: d minus the negatives */
             static_for<d>([&](auto E) {
-                acc ^= __float_as_uint(canon(P[edge_var<R, ZT, I, E>(r, a)]));
+                odd = odd != (*post_ptr<R, ZT, I, E>(P, Pr, Prz, r, a) < 0.0f);
             });
-            fail |= acc >> 31;
+            fail |= odd ? 1u : 0u;
         });
         return fail;
     };
@@ -199,14 +230,14 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
                 float L[d];
                 uint32_t LC[d];
                 uint32_t sgn = 0;
-                float m1 = 10000.0f, m2 = 10000.0f;
+                float m1, m2;
                 const float oM1 = M1[I], oM2 = M2[I];
                 const uint32_t oNeg = NEG[I];
                 const int oIdx = (int)(oNeg >> 27);
                 /* pass 1: L = post - old message, sign bits, two minima */
                 static_for<d>([&](auto E) {
                     constexpr int e = decltype(E)::value;
-                    const float x = P[edge_var<R, ZT, I, e>(r, a)];
+                    const float x = *post_ptr<R, ZT, I, e>(P, Pr, Prz, r, a);
                     const float mag = (oIdx == e) ? oM2 : oM1;
                     const uint32_t sb = (oNeg << (32 - d + e)) & 0x80000000u;
                     const float msg = __uint_as_float(__float_as_uint(mag) | sb);
@@ -214,10 +245,10 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
                     L[e] = l;
                     LC[e] = __float_as_uint(canon(l));
                     sgn = __funnelshift_l(LC[e], sgn, 1);
-                    const float al = fabsf(l);
-                    m2 = fminf(m2, fmaxf(m1, al));
-                    m1 = fminf(m1, al);
                 });
+                two_min_abs<0, d>(L, m1, m2);
+                m1 = fminf(m1, 10000.0f);
+                m2 = fminf(m2, 10000.0f);
                 /* bit (d-1-e) of sgn is neg(L_e); message e is negative iff
                  * (d & 1) ^ parity(neg) ^ neg(L_e)  (reference :148,172,191) */
                 const uint32_t flip = (uint32_t)((d & 1) ^ (__popc(sgn) & 1));
@@ -233,7 +264,7 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
                         nIdx = is_min ? e : nIdx;
                         const uint32_t sb = (LC[e] & 0x80000000u) ^ fb;
                         const float t = __uint_as_float(__float_as_uint(mu) | sb);
-                        P[edge_var<R, ZT, I, e>(r, a)] = __fadd_rn(l, t);
+                        *post_ptr<R, ZT, I, e>(P, Pr, Prz, r, a) = __fadd_rn(l, t);
                     });
                     M1[I] = m1;
                     M2[I] = m2;
@@ -260,7 +291,7 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
                         const int lo = is_min ? l2 : l1;
                         hi ^= (int)(LC[e] & 0x80000000u);
                         const double t = __hiloint2double(hi, lo);
-                        P[edge_var<R, ZT, I, e>(r, a)] = __double2float_rn(__dadd_rn((double)l, t));
+                        *post_ptr<R, ZT, I, e>(P, Pr, Prz, r, a) = __double2float_rn(__dadd_rn((double)l, t));
                     });
                     M1[I] = __double2float_rn(D1);
                     M2[I] = __double2float_rn(D2);

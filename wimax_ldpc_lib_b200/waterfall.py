@@ -2,6 +2,8 @@
 
   python -m wimax_ldpc_lib_b200.waterfall --z 96 48 [--rates 0 1 2 3 4 5] [--out results/waterfall.json]
 
+Writes the JSON result and the same points as CSV beside it (results/waterfall.csv).
+
 Frames are generated, encoded, modulated, corrupted and decoded on the
 device (framegen, or null-space codewords for 3/4B, which has no
 dual-diagonal encoder). For every (rate, z) and decoder (plain normalized
@@ -136,13 +138,31 @@ def ebno_at(points, target=1e-5):
     return None
 
 
+def pilot_frames(n):
+    """BER_example's pilot run: 46080 bits in whole frames (reference lib/BER_example.cc:142-150)."""
+    return max(1, 46080 // n)
+
+
+def ber_example_frames(pilot_ber, n):
+    """Frames of BER_example's main run after a pilot that measured pilot_ber:
+    10 * floor(3.912 / BER) bits, or floor(3.912 / 1e-8) bits when the pilot
+    saw no error, in whole frames (reference lib/BER_example.cc:152-166)."""
+    bits = math.floor(3.912 / 1e-8) if pilot_ber == 0.0 else 10 * math.floor(3.912 / pilot_ber)
+    return bits // n
+
+
+def capacity_frames(n):
+    """Frames per Eb/N0 step of the capacity search: 3.912 / 1e-5 bits over
+    n, plus one (reference lib/Capacity_plot_example.cc:150-160)."""
+    return int(3.912 / 0.00001) // n + 1
+
+
 def ber_example_point(rate, z, dec, ebno):
     """BER_example's procedure at one Eb/N0 (reference lib/BER_example.cc:142-169)."""
     src = FrameSource(rate, z, 1 << 17)
-    tot = run_frames(src, dec, ebno, max(1, 46080 // src.n))
+    tot = run_frames(src, dec, ebno, pilot_frames(src.n))
     ber = tot["cw_bit_errors"] / (tot["frames"] * src.k)
-    num_req = math.floor(3.912 / 1e-8) if ber == 0.0 else 10 * math.floor(3.912 / ber)
-    t2 = run_frames(src, dec, ebno, num_req // src.n)
+    t2 = run_frames(src, dec, ebno, ber_example_frames(ber, src.n))
     for key in tot:
         tot[key] += t2[key]
     return tot["cw_bit_errors"] / (tot["frames"] * src.k), tot["frames"]
@@ -151,7 +171,7 @@ def ber_example_point(rate, z, dec, ebno):
 def capacity_search(rate, z, dec, start=0.25, step=0.01, max_steps=2000):
     """Capacity_example's search (reference lib/Capacity_plot_example.cc:91,150-186)."""
     src = FrameSource(rate, z, 1 << 16)
-    frames = int(3.912 / 0.00001) // src.n + 1
+    frames = capacity_frames(src.n)
     eb = start
     for _ in range(max_steps):
         tot = run_frames(src, dec, eb, frames)
@@ -159,6 +179,22 @@ def capacity_search(rate, z, dec, start=0.25, step=0.01, max_steps=2000):
             return round(eb, 4)
         eb += step
     return None
+
+
+CSV_FIELDS = ["rate", "z", "decoder", "ebno_db", "frames", "fer", "ber", "bit_errors", "ber_reference_definition",
+              "mean_iterations", "info_gbps"]
+
+
+def write_csv(res, path):
+    """One line per (code, decoder, Eb/N0 point): the sweep as a table, in
+    place of the reference's MathGL plots."""
+    with open(path, "w") as f:
+        f.write(",".join(CSV_FIELDS) + "\n")
+        for e in res["codes"]:
+            for name, d in e["decoders"].items():
+                for p in d["points"]:
+                    row = {"rate": e["rate"], "z": e["z"], "decoder": name, **p}
+                    f.write(",".join(str(row[k]) for k in CSV_FIELDS) + "\n")
 
 
 def learned_weights(rate, z):
@@ -203,6 +239,7 @@ def main():
     os.makedirs(os.path.dirname(args.out), exist_ok=True)
     with open(args.out, "w") as f:
         json.dump(res, f, indent=1)
+    write_csv(res, os.path.splitext(args.out)[0] + ".csv")
     print("Eb/N0 at BER 1e-5:")
     for e in res["codes"]:
         print(f"  {e['rate']:5s} z={e['z']:3d}  " + "  ".join(
