@@ -58,16 +58,21 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def load_traffic(name):
-    """dram bytes per launch recorded from an ncu capture (profiles/<name>)."""
+def load_profile_value(name, key):
+    """a figure recorded from an ncu capture (profiles/<name>, line "key: value ...")."""
     p = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(p):
-            if line.startswith("traffic_bytes_per_launch_full_batch:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1].split()[0])
     except OSError:
         pass
     return None
+
+
+def load_traffic(name):
+    """dram bytes per launch of the full batch, from an ncu capture."""
+    return load_profile_value(name, "traffic_bytes_per_launch_full_batch")
 
 
 class ClockSampler:
@@ -342,7 +347,19 @@ def run_ours(args):
                 if head == "plain" else "lms_decode_kernel<0,96>",
                 "algorithmic_bytes_per_launch": bytes_per_launch,
                 "note": "5n bytes per frame (float32 LLR read + int8 hard-decision write); the decoders are "
-                        "instruction-issue bound, not HBM-bound (see DESIGN.md)"}
+                        "instruction-issue bound, not HBM-bound: see the issue roofline"}
+    # issue roofline: warp-instructions per frame (ncu, same workload) x frames
+    # per launch / launch time, against 4 issue slots per SM per cycle at the
+    # SM clock sampled during the timed region
+    prof = "tdmp_nms_r12_z96.txt" if head == "plain" else "lms_r12_z96.txt"
+    ipf = load_profile_value(prof, "warp_instructions_per_frame")
+    if ipf and clocks.get("sm_mhz"):
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        ach = ipf * frames / (ms * 1e-3)
+        pk = sms * 4 * clocks["sm_mhz"] * 1e6
+        roofline["issue"] = {"bound": "issue", "achieved": ach, "peak": pk, "unit": "warp-instructions/s",
+                             "frac": ach / pk, "warp_instructions_per_frame": ipf,
+                             "peak_basis": f"{sms} SMs x 4 schedulers x {clocks['sm_mhz']:.0f} MHz (sampled)"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

