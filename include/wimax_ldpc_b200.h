@@ -224,6 +224,20 @@ WLDPC_API int wldpc_lms_loss_grad(wldpc_lms* h, const float* llr, const uint8_t*
  * loss_history (nullable) receives the batch loss of every step. */
 WLDPC_API int wldpc_lms_train(wldpc_lms* h, unsigned steps, unsigned batch, float ebno_lo_db, float ebno_hi_db,
                               uint64_t seed, uint64_t first_frame, float lr, float* loss_history);
+/* One training step split in two, for data-parallel training over several
+ * GPUs (no counterpart in the reference): wldpc_lms_step_grad generates
+ * `batch` frames from counter first_frame as wldpc_lms_train does, runs the
+ * forward and backward passes and writes the batch's gradient (float[nw] on
+ * the device, compact [2][T][blocks] layout, nw from wldpc_lms_grad_size)
+ * and its loss (float on the device, nullable) without changing the weights;
+ * wldpc_lms_apply_grad applies one Adam step (as wldpc_lms_train) with a
+ * given device gradient, e.g. the mean of the ranks' gradients after an
+ * all-reduce. Both start after the work queued on `stream` and return when
+ * their results are complete. Calls on one handle must not overlap. */
+WLDPC_API int wldpc_lms_grad_size(wldpc_lms* h, size_t* nw);
+WLDPC_API int wldpc_lms_step_grad(wldpc_lms* h, unsigned batch, float ebno_lo_db, float ebno_hi_db, uint64_t seed,
+                                  uint64_t first_frame, float* grad, float* loss, void* stream);
+WLDPC_API int wldpc_lms_apply_grad(wldpc_lms* h, const float* grad, float lr, void* stream);
 
 /* ------------------------------------------------- allocation-free decode */
 

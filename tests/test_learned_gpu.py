@@ -88,3 +88,33 @@ def test_shipped_weights_gain_over_plain(wl, cuda):
         res[name] = (fer, (st & 0xFFFF).double().mean().item())
     assert res["learned"][0] <= res["plain8"][0], res
     assert res["learned"][1] < res["plain8"][1], res
+
+
+def test_split_training_step_equals_train(wl, cuda):
+    """wldpc_lms_step_grad + wldpc_lms_apply_grad (the data-parallel pieces)
+    give bit-identical weights to wldpc_lms_train on the same frames."""
+    torch = cuda
+    a, b = wl.LearnedDecoder(0, 24, 8), wl.LearnedDecoder(0, 24, 8)
+    g = torch.zeros(b.grad_size(), dtype=torch.float32, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+    for s in range(3):
+        a.train(1, 256, 1.0, 3.0, 17, first_frame=s * 256, lr=1e-2)
+        b.step_grad(256, 1.0, 3.0, 17, s * 256, g, loss)
+        b.apply_grad(g, 1e-2)
+    assert np.array_equal(a.get_weights(), b.get_weights())
+    assert float(loss.item()) > 0
+
+
+def test_rank_gradients_average_to_the_job_gradient(wl, cuda):
+    """Two ranks' half batches (frames [0, 256) and [256, 512)) average to the
+    gradient of the whole batch, as the all-reduce in data-parallel training
+    assumes (float sums in a different order: 1e-5 relative)."""
+    torch = cuda
+    h = wl.LearnedDecoder(0, 48, 8)
+    n = h.grad_size()
+    full, r0, r1 = (torch.zeros(n, dtype=torch.float32, device="cuda") for _ in range(3))
+    h.step_grad(512, 1.0, 3.0, 5, 0, full)
+    h.step_grad(256, 1.0, 3.0, 5, 0, r0)
+    h.step_grad(256, 1.0, 3.0, 5, 256, r1)
+    avg = (r0 + r1) / 2
+    assert torch.linalg.norm(avg - full) <= 1e-5 * torch.linalg.norm(full)

@@ -89,6 +89,10 @@ def _lib():
     L.wldpc_lms_loss_grad.argtypes = [_p, _p, _p, _sz, _p, ctypes.POINTER(ctypes.c_double)]
     L.wldpc_lms_train.argtypes = [_p, _u, _u, ctypes.c_float, ctypes.c_float, ctypes.c_uint64, ctypes.c_uint64,
                                   ctypes.c_float, _p]
+    L.wldpc_lms_grad_size.argtypes = [_p, ctypes.POINTER(_sz)]
+    L.wldpc_lms_step_grad.argtypes = [_p, _u, ctypes.c_float, ctypes.c_float, ctypes.c_uint64, ctypes.c_uint64, _p,
+                                      _p, _p]
+    L.wldpc_lms_apply_grad.argtypes = [_p, _p, ctypes.c_float, _p]
     L.wldpc_decode_host_noalloc.argtypes = [_i, _u, _u, _p, _p, _p, _sz]
     L.wldpc_lfsr_bits_device.argtypes = [ctypes.c_uint64, _sz, _p, _p]
     L.wldpc_framegen_nullspace_device.argtypes = [_i, _u, ctypes.c_uint64, ctypes.c_uint64, _sz, ctypes.c_float,
@@ -406,6 +410,23 @@ class LearnedDecoder:
         _check(_lib().wldpc_lms_train(self._h, steps, batch, ebno_lo, ebno_hi, seed, first_frame, lr,
                                       _np_ptr(hist)), "lms train")
         return hist[:steps]
+
+    def grad_size(self) -> int:
+        nw = ctypes.c_size_t()
+        _check(_lib().wldpc_lms_grad_size(self._h, ctypes.byref(nw)), "grad_size")
+        return nw.value
+
+    def step_grad(self, batch: int, ebno_lo: float, ebno_hi: float, seed: int, first_frame: int, grad, loss=None,
+                  stream=None):
+        """Gradient of one generated batch into `grad` (float32 CUDA tensor of
+        grad_size() values) and its loss into `loss` (one float32, optional);
+        the weights do not change."""
+        _check(_lib().wldpc_lms_step_grad(self._h, batch, ebno_lo, ebno_hi, seed, first_frame, _t_ptr(grad),
+                                          _t_ptr(loss), _stream_ptr(stream)), "lms step_grad")
+
+    def apply_grad(self, grad, lr: float = 1e-3, stream=None):
+        """One Adam step with the gradient in `grad` (float32 CUDA tensor)."""
+        _check(_lib().wldpc_lms_apply_grad(self._h, _t_ptr(grad), lr, _stream_ptr(stream)), "lms apply_grad")
 
 
 class BERRunner:

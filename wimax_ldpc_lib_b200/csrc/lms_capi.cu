@@ -111,6 +111,7 @@ struct wldpc_lms {
     Buf ckp, ckm, gpart, lpart, tllr, tcw;             /* training scratch */
     Buf pllr[2], phard[2], pstat[2];                   /* host-batch pipeline staging */
     cudaStream_t pipe[2] = {nullptr, nullptr};
+    cudaEvent_t ev_user = nullptr;                     /* orders the handle's stream after a caller's */
     int adam_step = 0;
 };
 
@@ -194,6 +195,7 @@ int wldpc_lms_destroy(wldpc_lms* h)
             cudaStreamDestroy(ps);
         }
     if (h->err) cudaFree(h->err);
+    if (h->ev_user) cudaEventDestroy(h->ev_user);
     delete h;
     return WLDPC_OK;
 }
@@ -450,6 +452,91 @@ int wldpc_lms_train(wldpc_lms* h, unsigned steps, unsigned batch, float ebno_lo_
     if (loss_history && steps) CU(cudaMemcpyAsync(loss_history, h->loss.p, (size_t)steps * 4, cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     return lms_sync_host_weights(h);
+}
+
+/* the handle's stream waits for the work the caller queued on `user` */
+static int lms_after_user_stream(wldpc_lms* h, cudaStream_t user)
+{
+    if (!h->ev_user) CU(cudaEventCreateWithFlags(&h->ev_user, cudaEventDisableTiming));
+    CU(cudaEventRecord(h->ev_user, user));
+    CU(cudaStreamWaitEvent(h->stream, h->ev_user, 0));
+    return WLDPC_OK;
+}
+
+int wldpc_lms_grad_size(wldpc_lms* h, size_t* nw)
+{
+    if (!h || !nw) return WLDPC_ERR_ARG;
+    *nw = (size_t)2 * h->T * h->nblk;
+    return WLDPC_OK;
+}
+
+int wldpc_lms_step_grad(wldpc_lms* h, unsigned batch, float ebno_lo_db, float ebno_hi_db, uint64_t seed,
+                        uint64_t first_frame, float* grad, float* loss, void* stream)
+{
+    if (!h || batch == 0 || !grad) return WLDPC_ERR_ARG;
+    if (h->host_stale == false) {
+        int rc = lms_push_device_weights(h);
+        if (rc) return rc;
+    }
+    const size_t n = (size_t)h->code.n, nw = (size_t)2 * h->T * h->nblk;
+    int rc;
+    if ((rc = h->tllr.reserve((size_t)batch * n * 4)) || (rc = h->tcw.reserve((size_t)batch * n)) ||
+        (rc = h->loss.reserve(4)))
+        return rc;
+    if ((rc = lms_after_user_stream(h, (cudaStream_t)stream))) return rc;
+    FramegenArgs f{};
+    f.seed = seed;
+    f.first_frame = first_frame;
+    f.frames = batch;
+    f.ebno_lo = ebno_lo_db;
+    f.ebno_hi = ebno_hi_db;
+    f.cw = (uint8_t*)h->tcw.p;
+    f.llr = (float*)h->tllr.p;
+    if (h->rate == THREEQUARTERSB) {
+        if ((rc = wldpc_internal_nullspace_frames(h->rate, h->z, f, h->stream))) return rc;
+    } else {
+        CU(launch_framegen(h->code, f, h->stream));
+    }
+    if ((rc = lms_forward_backward(h, (const float*)h->tllr.p, (const uint8_t*)h->tcw.p, batch, h->stream)))
+        return rc;
+    if ((rc = lms_reduce(h, batch, 0, 0.0f, (float*)h->loss.p, h->stream))) return rc;
+    CU(cudaMemcpyAsync(grad, h->grad.p, nw * 4, cudaMemcpyDeviceToDevice, h->stream));
+    if (loss) CU(cudaMemcpyAsync(loss, h->loss.p, 4, cudaMemcpyDeviceToDevice, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    return WLDPC_OK;
+}
+
+int wldpc_lms_apply_grad(wldpc_lms* h, const float* grad, float lr, void* stream)
+{
+    if (!h || !grad) return WLDPC_ERR_ARG;
+    if (h->host_stale == false) {
+        int rc = lms_push_device_weights(h);
+        if (rc) return rc;
+    }
+    int rc;
+    if ((rc = lms_after_user_stream(h, (cudaStream_t)stream))) return rc;
+    AdamArgs a;
+    a.gpart = grad;            /* one "frame": the given gradient */
+    a.loss_part = nullptr;
+    a.grad = (float*)h->grad.p;
+    a.w = (float*)h->wdev.p;
+    a.m = (float*)h->mdev.p;
+    a.v = (float*)h->vdev.p;
+    a.loss_out = nullptr;
+    a.frames = 1;
+    a.nw = 2 * h->T * h->nblk;
+    a.step = h->adam_step + 1;
+    a.lr = lr;
+    a.beta1 = 0.9f;
+    a.beta2 = 0.999f;
+    a.eps = 1e-8f;
+    a.apply = 1;
+    lms_reduce_adam_kernel<<<(a.nw + 127) / 128, 128, 0, h->stream>>>(a);
+    CU(cudaGetLastError());
+    h->adam_step++;
+    h->host_stale = true;
+    CU(cudaStreamSynchronize(h->stream));
+    return WLDPC_OK;
 }
 
 }  // extern "C"
