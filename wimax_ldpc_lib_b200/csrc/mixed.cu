@@ -140,9 +140,12 @@ __device__ __forceinline__ void mixed_run_item(const MixedArgs& a, const MixedIt
                 const float oM1 = M1[I], oM2 = M2[I];
                 const uint32_t oNeg = NEG[I];
                 const int oIdx = (int)(oNeg >> 27);
+                /* the layer's edge addresses, loaded once for both passes */
+                int ad[d];
+                static_for<d>([&](auto E_) { ad[decltype(E_)::value] = mixed_var<R, I, decltype(E_)::value, THREADS>(A); });
                 static_for<d>([&](auto E_) {
                     constexpr int e = decltype(E_)::value;
-                    const float x = P[mixed_var<R, I, e, THREADS>(A)];
+                    const float x = P[ad[e]];
                     const float mag = (oIdx == e) ? oM2 : oM1;
                     const uint32_t sb = (oNeg << (32 - d + e)) & 0x80000000u;
                     const float l = __fsub_rn(x, __uint_as_float(__float_as_uint(mag) | sb));
@@ -170,8 +173,7 @@ __device__ __forceinline__ void mixed_run_item(const MixedArgs& a, const MixedIt
                     int hi = is_min ? h2 : h1;
                     const int lo = is_min ? l2 : l1;
                     hi ^= (int)(LC[e] & 0x80000000u);
-                    P[mixed_var<R, I, e, THREADS>(A)] =
-                        __double2float_rn(__dadd_rn((double)l, __hiloint2double(hi, lo)));
+                    P[ad[e]] = __double2float_rn(__dadd_rn((double)l, __hiloint2double(hi, lo)));
                 });
                 M1[I] = __double2float_rn(D1);
                 M2[I] = __double2float_rn(D2);

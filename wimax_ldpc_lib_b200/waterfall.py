@@ -197,6 +197,13 @@ def write_csv(res, path):
                     f.write(",".join(str(row[k]) for k in CSV_FIELDS) + "\n")
 
 
+def save(res, out):
+    os.makedirs(os.path.dirname(os.path.abspath(out)), exist_ok=True)
+    with open(out, "w") as f:
+        json.dump(res, f, indent=1)
+    write_csv(res, os.path.splitext(out)[0] + ".csv")
+
+
 def learned_weights(rate, z):
     p = os.path.join(HERE, "weights", f"lms_r{rate}_z{z}_T8.json")
     if not os.path.exists(p):
@@ -235,11 +242,8 @@ def main():
             if args.capacity and rate != 4:
                 entry["capacity_search_ebno_db"] = capacity_search(rate, z, decs["plain"])
             res["codes"].append(entry)
-    res["seconds"] = round(time.time() - t0, 1)
-    os.makedirs(os.path.dirname(args.out), exist_ok=True)
-    with open(args.out, "w") as f:
-        json.dump(res, f, indent=1)
-    write_csv(res, os.path.splitext(args.out)[0] + ".csv")
+            res["seconds"] = round(time.time() - t0, 1)
+            save(res, args.out)   # after every code, so a partial sweep is kept
     print("Eb/N0 at BER 1e-5:")
     for e in res["codes"]:
         print(f"  {e['rate']:5s} z={e['z']:3d}  " + "  ".join(
