@@ -250,7 +250,8 @@ static int lms_launch_decode(wldpc_lms* h, const float* llr, int8_t* hard, float
     a.frames = (long long)frames;
     a.iters = h->cap;
     a.wrows = h->T;
-    a.w = h->w;
+    for (int t = 0; t < h->T; t++)
+        for (int b = 0; b < h->nblk; b++) a.wab[t][b] = make_float2(h->w.a[t][b], h->w.b[t][b]);
     const LmsLaunch* k = h->k;
     if (k->smem > 48 * 1024)
         CU(cudaFuncSetAttribute(k->decode, cudaFuncAttributeMaxDynamicSharedMemorySize, k->smem));
