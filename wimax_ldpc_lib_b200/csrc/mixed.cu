@@ -189,9 +189,12 @@ __device__ __forceinline__ void mixed_run_item(const MixedArgs& a, const MixedIt
 }
 
 /* One persistent kernel per rate: it takes work items of its rate from its
- * own queue until none are left. */
+ * own queue until none are left. The register cap (80 per thread: 8 CTAs of
+ * 96 or 4 of 192 threads per SM) trades a few spills in the 5/6 kernels for
+ * more resident warps; the kernel is latency-bound, and this measured 18.6
+ * against 16.2 info Gbit/s uncapped on the mixed batch. */
 template <int R, int THREADS>
-__global__ void __launch_bounds__(THREADS) mixed_decode_kernel(const __grid_constant__ MixedArgs a)
+__global__ void __launch_bounds__(THREADS, (THREADS == 96 ? 8 : 4)) mixed_decode_kernel(const __grid_constant__ MixedArgs a)
 {
     extern __shared__ __align__(16) float smem_mixed[];   /* posteriors, then the address table */
     __shared__ MixedSlots S;
