@@ -88,3 +88,38 @@ def test_no_device_fails_loudly(wl):
     assert wl.lib().wldpc_decoder_create(0, 96, 10, 1, 0, ctypes.byref(h)) == wl.ERR_NO_DEVICE
     with pytest.raises(wl.LdpcError):
         wl.Decoder(0, 96)
+
+
+def test_argument_checks_of_the_additions(wl):
+    """Entry points with no reference counterpart (learned decoder and its
+    data-parallel pieces, mixed batch, allocation-free decode) reject bad
+    arguments before touching a device."""
+    L = wl.lib()
+    h = ctypes.c_void_p()
+    nw = ctypes.c_size_t()
+    # learned decoder: codes, iteration count, supported z (24, 48, 96)
+    assert L.wldpc_lms_create(6, 96, 8, ctypes.byref(h)) == wl.ERR_CODE
+    assert L.wldpc_lms_create(0, 97, 8, ctypes.byref(h)) == wl.ERR_CODE
+    assert L.wldpc_lms_create(0, 96, 0, ctypes.byref(h)) == wl.ERR_ARG
+    assert L.wldpc_lms_create(0, 96, 9, ctypes.byref(h)) == wl.ERR_ARG
+    assert L.wldpc_lms_create(0, 36, 8, ctypes.byref(h)) == wl.ERR_UNSUPPORTED
+    assert L.wldpc_lms_create(0, 96, 8, None) == wl.ERR_ARG
+    assert L.wldpc_lms_destroy(None) == wl.ERR_ARG
+    assert L.wldpc_lms_grad_size(None, ctypes.byref(nw)) == wl.ERR_ARG
+    assert L.wldpc_lms_step_grad(None, 16, 1.0, 2.0, 1, 0, None, None, None) == wl.ERR_ARG
+    assert L.wldpc_lms_apply_grad(None, None, 1e-3, None) == wl.ERR_ARG
+    # mixed batch: variant numbering rate * 19 + (z - 24) / 4, bad codes, bad caps
+    assert L.wldpc_variant(0, 24) == 0 and L.wldpc_variant(0, 96) == 18 and L.wldpc_variant(5, 96) == 113
+    assert L.wldpc_variant(6, 96) == wl.ERR_CODE and L.wldpc_variant(0, 26) == wl.ERR_CODE
+    assert L.wldpc_mixed_create(0x10000, ctypes.byref(h)) == wl.ERR_ARG
+    assert L.wldpc_mixed_create(10, None) == wl.ERR_ARG
+    assert L.wldpc_mixed_destroy(None) == wl.ERR_ARG
+    assert L.wldpc_mixed_set_config(None, 96, 32) == wl.ERR_ARG
+    # allocation-free decode: code, cap and the scratch limit come before any device call
+    assert L.wldpc_decode_host_noalloc(0, 100, 10, None, None, None, 1) == wl.ERR_CODE
+    assert L.wldpc_decode_host_noalloc(0, 96, 0x10000, None, None, None, 1) == wl.ERR_ARG
+    assert L.wldpc_decode_host_noalloc(0, 96, 10, None, None, None, 0) == 0
+    buf = np.zeros(2304, np.float32)
+    out = np.zeros(2304, np.int8)
+    assert L.wldpc_decode_host_noalloc(0, 96, 10, ctypes.c_void_p(buf.ctypes.data), ctypes.c_void_p(out.ctypes.data),
+                                       None, 91) == -7   # WLDPC_ERR_SCRATCH: 90 frames of z=96 at most
