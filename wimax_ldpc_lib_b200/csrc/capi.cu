@@ -74,10 +74,10 @@ struct wldpc_decoder {
     unsigned max_iter;
     CodeDesc code;
     cudaStream_t stream = nullptr;
-    cudaStream_t pipe[2] = {nullptr, nullptr};
+    cudaStream_t pipe[kHostStages] = {};
     unsigned* err = nullptr;   /* device error word */
     DevBuf llr, hard, status, bits;
-    DevBuf pllr[2], phard[2], pstatus[2];
+    DevBuf pllr[kHostStages], phard[kHostStages], pstatus[kHostStages];
 };
 
 struct wldpc_encoder {
@@ -369,9 +369,9 @@ int wldpc_decode_batch_host(wldpc_decoder* d, float* rx, int8_t* decoded, uint32
     if (!d || (frames && (!rx || !decoded))) return WLDPC_ERR_ARG;
     if (frames == 0) return WLDPC_OK;
     const size_t n = (size_t)d->code.n;
-    const size_t chunk = frames < 32768 ? frames : 32768;
+    const size_t chunk = frames < kHostChunk ? frames : kHostChunk;
     int rc;
-    for (int s = 0; s < 2; s++) {
+    for (int s = 0; s < kHostStages; s++) {
         if (!d->pipe[s]) CU(cudaStreamCreateWithFlags(&d->pipe[s], cudaStreamNonBlocking));
         if ((rc = d->pllr[s].reserve(chunk * n * 4)) || (rc = d->phard[s].reserve(chunk * n)) ||
             (rc = d->pstatus[s].reserve(chunk * 4)))
@@ -385,7 +385,7 @@ int wldpc_decode_batch_host(wldpc_decoder* d, float* rx, int8_t* decoded, uint32
     }
     size_t idx = 0;
     for (size_t f0 = 0; f0 < frames; f0 += chunk, idx++) {
-        const int s = (int)(idx & 1);
+        const int s = (int)(idx % kHostStages);
         const size_t nf = frames - f0 < chunk ? frames - f0 : chunk;
         cudaStream_t st = d->pipe[s];
         CU(cudaMemcpyAsync(d->pllr[s].p, rx + f0 * n, nf * n * 4, cudaMemcpyHostToDevice, st));
@@ -396,8 +396,7 @@ int wldpc_decode_batch_host(wldpc_decoder* d, float* rx, int8_t* decoded, uint32
         CU(cudaMemcpyAsync(decoded + f0 * n, d->phard[s].p, nf * n, cudaMemcpyDeviceToHost, st));
         if (st_host) CU(cudaMemcpyAsync(st_host + f0, d->pstatus[s].p, nf * 4, cudaMemcpyDeviceToHost, st));
     }
-    CU(cudaStreamSynchronize(d->pipe[0]));
-    CU(cudaStreamSynchronize(d->pipe[1]));
+    for (int s = 0; s < kHostStages; s++) CU(cudaStreamSynchronize(d->pipe[s]));
     if ((rc = read_err(d))) return rc;
     if (num_errors)
         for (size_t f = 0; f < frames; f++) num_errors[f] = ref_return(d, st_host[f]);

@@ -109,8 +109,8 @@ struct wldpc_lms {
     unsigned* err = nullptr;
     Buf wdev, mdev, vdev, grad, loss;                  /* training state: [2][T][nblk] */
     Buf ckp, ckm, gpart, lpart, tllr, tcw;             /* training scratch */
-    Buf pllr[2], phard[2], pstat[2];                   /* host-batch pipeline staging */
-    cudaStream_t pipe[2] = {nullptr, nullptr};
+    Buf pllr[kHostStages], phard[kHostStages], pstat[kHostStages];                   /* host-batch pipeline staging */
+    cudaStream_t pipe[kHostStages] = {};
     cudaEvent_t ev_user = nullptr;                     /* orders the handle's stream after a caller's */
     int adam_step = 0;
 };
@@ -286,9 +286,9 @@ int wldpc_lms_decode_host(wldpc_lms* h, float* rx, int8_t* decoded, uint32_t* nu
     if (!h || (frames && (!rx || !decoded))) return WLDPC_ERR_ARG;
     if (frames == 0) return WLDPC_OK;
     const size_t n = (size_t)h->code.n;
-    const size_t chunk = frames < 32768 ? frames : 32768;
+    const size_t chunk = frames < kHostChunk ? frames : kHostChunk;
     int rc;
-    for (int s = 0; s < 2; s++) {
+    for (int s = 0; s < kHostStages; s++) {
         if (!h->pipe[s]) CU(cudaStreamCreateWithFlags(&h->pipe[s], cudaStreamNonBlocking));
         if ((rc = h->pllr[s].reserve(chunk * n * 4)) || (rc = h->phard[s].reserve(chunk * n)) ||
             (rc = h->pstat[s].reserve(chunk * 4)))
@@ -302,7 +302,7 @@ int wldpc_lms_decode_host(wldpc_lms* h, float* rx, int8_t* decoded, uint32_t* nu
     }
     size_t idx = 0;
     for (size_t f0 = 0; f0 < frames; f0 += chunk, idx++) {
-        const int s = (int)(idx & 1);
+        const int s = (int)(idx % kHostStages);
         const size_t nf = frames - f0 < chunk ? frames - f0 : chunk;
         cudaStream_t ps = h->pipe[s];
         CU(cudaMemcpyAsync(h->pllr[s].p, rx + f0 * n, nf * n * 4, cudaMemcpyHostToDevice, ps));
@@ -313,8 +313,7 @@ int wldpc_lms_decode_host(wldpc_lms* h, float* rx, int8_t* decoded, uint32_t* nu
         CU(cudaMemcpyAsync(decoded + f0 * n, h->phard[s].p, nf * n, cudaMemcpyDeviceToHost, ps));
         if (st) CU(cudaMemcpyAsync(st + f0, h->pstat[s].p, nf * 4, cudaMemcpyDeviceToHost, ps));
     }
-    CU(cudaStreamSynchronize(h->pipe[0]));
-    CU(cudaStreamSynchronize(h->pipe[1]));
+    for (int s = 0; s < kHostStages; s++) CU(cudaStreamSynchronize(h->pipe[s]));
     unsigned e = 0;
     CU(cudaMemcpy(&e, h->err, 4, cudaMemcpyDeviceToHost));
     if (e) {
