@@ -361,8 +361,9 @@ int wldpc_syndrome_batch_host(wldpc_decoder* d, const int8_t* bits, int exit_ear
     return WLDPC_OK;
 }
 
-/* Host batch: chunks alternate between two streams so that the copy-in of
- * one chunk, the kernel of another and the copy-out of a third overlap. */
+/* Host batch: chunks of kHostChunk frames rotate over kHostStages streams so
+ * that the copy-in of one chunk, the kernel of another and the copy-out of a
+ * third overlap. */
 int wldpc_decode_batch_host(wldpc_decoder* d, float* rx, int8_t* decoded, uint32_t* num_errors,
                             int32_t* status, size_t frames)
 {
@@ -633,10 +634,12 @@ int wldpc_lfsr_bits_device(uint64_t first_bit, size_t nbits, uint8_t* out, void*
     if (nbits && !out) return WLDPC_ERR_ARG;
     int rc = check_device();
     if (rc) return rc;
-    static bool uploaded[64] = {false};
+    static bool uploaded[64] = {false};   /* per device: the period table is in place */
+    static std::mutex upload_mutex;
     int dev = 0;
     CU(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return WLDPC_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(upload_mutex);
     if (!uploaded[dev]) {
         /* one period of the stream, as BER_runner::lfsr_get_num produces it */
         std::vector<uint32_t> words(115200 / 32, 0u);

@@ -278,7 +278,7 @@ int wldpc_lms_set_cap(wldpc_lms* h, unsigned cap)
     return WLDPC_OK;
 }
 
-/* Host batch: chunks alternate between two streams so that copies and
+/* Host batch: chunks rotate over kHostStages streams so that copies and
  * kernels of neighbouring chunks overlap (as wldpc_decode_batch_host). */
 int wldpc_lms_decode_host(wldpc_lms* h, float* rx, int8_t* decoded, uint32_t* num_errors, int32_t* status,
                           size_t frames)

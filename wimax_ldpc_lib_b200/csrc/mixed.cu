@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 #include <cuda_runtime.h>
@@ -294,7 +295,9 @@ struct MBuf {
     }
 };
 
+/* per device: the code table has been copied into c_codes */
 bool g_codes_uploaded[64] = {false};
+std::mutex g_codes_mutex;
 
 int upload_codes()
 {
@@ -304,6 +307,7 @@ int upload_codes()
         return WLDPC_ERR_NO_DEVICE;
     }
     if (dev < 0 || dev >= 64) return WLDPC_ERR_UNSUPPORTED;
+    std::lock_guard<std::mutex> lock(g_codes_mutex);
     if (g_codes_uploaded[dev]) return WLDPC_OK;
     std::vector<MixedCode> t(kVariants);
     for (int rate = 0; rate < kRates; rate++)
