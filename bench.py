@@ -5,12 +5,13 @@ seeded synthetic frames (random info bits, the project's encoder, BPSK, AWGN,
 LLR = 2y/sigma^2) generated on the device at Eb/N0 = 2.25 dB, where the plain
 normalized min-sum decoder with the reference's cap of 10 iterations has
 FER <= 1e-3. A step decodes one batch of 262144 frames (2.4 GB of float32 LLRs,
-larger than L2, so no flush is needed between steps). Both decoders run on the
+larger than L2, so no flush is needed between steps). All decoders run on the
 same frames: the plain (bit-exact) decoder and, when trained weights are
 shipped, the learned min-sum decoder (8 trained iterations, run to the same
-cap of 10 with the last trained weights); `value` is the learned one's when
-its FER meets the target, is no worse than the plain decoder's and it is
-faster, else the plain one's; `decoders` reports both.
+cap of 10 with the last trained weights) in fp32 and in packed binary16 (two
+frames per thread); `value` is the fastest learned variant's whose FER meets
+the target, is no worse than the plain decoder's and that is faster, else the
+plain one's; `decoders` reports all three.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -250,6 +251,10 @@ def run_ours(args):
         # ones reuse the last trained weights), judged against plain at cap 10
         decoders["learned"] = wl.LearnedDecoder(RATE, Z, lms_meta["iterations"],
                                                 weights=np.array(lms_meta["weights"], np.float32), cap=MAX_ITER)
+        # the same network decoded in packed binary16, two frames per thread
+        decoders["learned_f16x2"] = wl.LearnedDecoder(RATE, Z, lms_meta["iterations"],
+                                                      weights=np.array(lms_meta["weights"], np.float32),
+                                                      cap=MAX_ITER, precision=wl.LMS_F16X2)
 
     def measure(dec):
         for _ in range(args.warmup):
@@ -290,13 +295,14 @@ def run_ours(args):
         if hasattr(dec, "synchronize"):
             dec.synchronize()
 
-    # the headline decoder: learned where it meets the FER target and is faster, else plain
+    # the headline decoder: the fastest learned variant that meets the FER
+    # target, is no worse than plain and is faster, else plain
     head = "plain"
-    if "learned" in results:
-        L, P = results["learned"], results["plain"]
-        # ships where it meets the target, is no worse than plain and is faster
-        if L["fer"] <= 1e-3 and L["fer"] <= P["fer"] and L["value"] > P["value"]:
-            head = "learned"
+    P = results["plain"]
+    for name in ("learned", "learned_f16x2"):
+        L = results.get(name)
+        if L and L["fer"] <= 1e-3 and L["fer"] <= P["fer"] and L["value"] > results[head]["value"]:
+            head = name
     R = results[head]
     ms = R["ms_per_step"]
     value = R["value"]
@@ -341,17 +347,19 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     bytes_per_launch = frames * 5 * n
     achieved = bytes_per_launch / (ms * 1e-3) / 1e9
-    traffic = load_traffic("tdmp_nms_r12_z96.txt" if head == "plain" else "lms_r12_z96.txt")
+    prof = {"plain": "tdmp_nms_r12_z96.txt", "learned": "lms_r12_z96.txt",
+            "learned_f16x2": "lms16_r12_z96.txt"}[head]
+    kernel = {"plain": "tdmp_decode_kernel<0,96,NMS>", "learned": "lms_decode_kernel<0,96>",
+              "learned_f16x2": "lms16_decode_kernel<0,96>"}[head]
+    traffic = load_traffic(prof)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_kind": peak_kind, "kernel": "tdmp_decode_kernel<0,96,NMS>"
-                if head == "plain" else "lms_decode_kernel<0,96>",
+                "traffic": traffic, "peak_kind": peak_kind, "kernel": kernel,
                 "algorithmic_bytes_per_launch": bytes_per_launch,
                 "note": "5n bytes per frame (float32 LLR read + int8 hard-decision write); the decoders are "
                         "instruction-issue bound, not HBM-bound: see the issue roofline"}
     # issue roofline: warp-instructions per frame (ncu, same workload) x frames
     # per launch / launch time, against 4 issue slots per SM per cycle at the
     # SM clock sampled during the timed region
-    prof = "tdmp_nms_r12_z96.txt" if head == "plain" else "lms_r12_z96.txt"
     ipf = load_profile_value(prof, "warp_instructions_per_frame")
     if ipf and clocks.get("sm_mhz"):
         sms = torch.cuda.get_device_properties(0).multi_processor_count
@@ -367,12 +375,15 @@ def run_ours(args):
         cpu = cpu_reference_baseline(llr[:n_sample].cpu().numpy())
 
     if rank == 0:
+        T = lms_meta["iterations"] if lms_meta else 8
         cfg_dec = {"plain": f"plain NMS TDMP (bit-exact), cap {MAX_ITER}",
-                   "learned": f"learned min-sum ({lms_meta['iterations'] if lms_meta else 8} trained iterations), "
-                              f"cap {MAX_ITER}"}
+                   "learned": f"learned min-sum ({T} trained iterations, fp32), cap {MAX_ITER}",
+                   "learned_f16x2": f"learned min-sum ({T} trained iterations, packed binary16, two frames per "
+                                    f"thread), cap {MAX_ITER}"}
         line = {"metric": METRIC, "value": value, "unit": "info Gbit/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f32" if head == "learned" else "f32+f64", "data": "synthetic",
+                "vs_baseline": None, "dtype": {"plain": "f32+f64", "learned": "f32", "learned_f16x2": "f16x2"}[head],
+                "data": "synthetic",
                 "config": {"workload": f"{cfg_dec[head]} decode, rate 1/2 z=96, {frames} frames per GPU per step, "
                                        f"Eb/N0 {EBNO_DB} dB",
                            "frames_per_gpu": frames, "ebno_db": EBNO_DB, "decoder": head,

@@ -206,6 +206,20 @@ WLDPC_API int wldpc_lms_get_weights(wldpc_lms* h, float* table);
 /* Iteration cap of decoding (default: the trained iterations T); iterations
  * past T use the weights of iteration T-1. */
 WLDPC_API int wldpc_lms_set_cap(wldpc_lms* h, unsigned cap);
+/* Inference arithmetic of the learned decoder (no counterpart in the
+ * reference, whose decoder has fixed constants). WLDPC_LMS_F32, the default,
+ * decodes in fp32. WLDPC_LMS_F16X2 decodes two frames per thread in packed
+ * IEEE binary16, about half the instructions per frame: every operation
+ * rounds to binary16, input LLRs are clamped to +-2048 and row minima to
+ * 2048, weights are rounded to binary16, and the posteriors returned are the
+ * exact float values of the binary16 results. A frame's outputs do not depend
+ * on the other frames of the batch. F16X2 needs |a| <= 2 and |b| <= 1024 for
+ * every weight, which keeps every sum finite; otherwise this call, or a
+ * decode after training moved a weight out of range, returns WLDPC_ERR_ARG.
+ * Training always runs in fp32. */
+#define WLDPC_LMS_F32 0
+#define WLDPC_LMS_F16X2 1
+WLDPC_API int wldpc_lms_set_precision(wldpc_lms* h, int precision);
 /* Decode on device buffers (layout and status as wldpc_decode_batch_device). */
 WLDPC_API int wldpc_lms_decode_device(wldpc_lms* h, const float* llr, int8_t* decoded, float* posterior,
                                       int32_t* status, size_t frames, void* stream);

@@ -84,6 +84,11 @@ class Oracle:
         L.wo_framegen.argtypes = [_i, _i, ctypes.c_uint64, ctypes.c_uint64, _l, ctypes.c_double,
                                   ctypes.c_double, _p, _p, _p, _p]
         L.wo_learned_decode_batch.argtypes = [_i, _i, _i, _i, _p, _l, _p, _p, _p, _p, _i]
+        L.wo_learned16_decode_batch.argtypes = [_i, _i, _i, _i, _p, _l, _p, _p, _p, _p, _p, _i]
+        L.wo_half_round.argtypes = [ctypes.c_double]
+        L.wo_half_round.restype = ctypes.c_double
+        L.wo_half_fma_relu.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.wo_half_fma_relu.restype = ctypes.c_double
         L.wo_learned_loss_grad.argtypes = [_i, _i, _i, _p, _l, _p, _p, _p]
         L.wo_learned_loss_grad.restype = ctypes.c_double
         self.threads = os.cpu_count() or 1
@@ -187,6 +192,27 @@ class Oracle:
                                             _ptr(dec), _ptr(it), _ptr(sf), threads or self.threads):
             raise ValueError("wo_learned_decode_batch failed")
         return post, dec, it, sf
+
+    def learned16_decode(self, rate, z, iterations, w, llr, threads=None, cap=None):
+        """The packed-half learned decoder restated per frame: (posterior, decoded,
+        iterations, synfail); llr is not modified."""
+        llr = np.ascontiguousarray(llr, np.float32)
+        w = np.ascontiguousarray(w, np.float32)
+        post = np.empty_like(llr)
+        dec = np.empty(llr.shape, np.int8)
+        it = np.empty(llr.shape[0], np.int32)
+        sf = np.empty(llr.shape[0], np.int32)
+        if self.lib.wo_learned16_decode_batch(rate, z, iterations, iterations if cap is None else cap, _ptr(w),
+                                              llr.shape[0], _ptr(llr), _ptr(post), _ptr(dec), _ptr(it), _ptr(sf),
+                                              threads or self.threads):
+            raise ValueError("wo_learned16_decode_batch failed")
+        return post, dec, it, sf
+
+    def half_round(self, x: float) -> float:
+        return self.lib.wo_half_round(float(x))
+
+    def half_fma_relu(self, a: float, b: float, c: float) -> float:
+        return self.lib.wo_half_fma_relu(float(a), float(b), float(c))
 
     def learned_loss_grad(self, rate, z, iterations, w, llr, cw):
         llr = np.ascontiguousarray(llr, np.float32)

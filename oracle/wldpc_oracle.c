@@ -468,6 +468,140 @@ int wo_learned_decode_batch(int rate, int z, int iterations, int cap, const floa
     return 0;
 }
 
+/* ------------------------------------- learned min-sum in binary16 lanes */
+
+/* Restates the packed-half learned decoder (wimax_ldpc_lib_b200/csrc/lms16.cuh)
+ * one frame at a time: every value is a binary16 number held exactly in a
+ * float, and every operation is computed exactly in double and rounded once
+ * to binary16 (nearest, ties to even). Sums and differences of two binary16
+ * numbers are exact in double; the fused multiply-add uses an exact TwoSum
+ * so that its single rounding is exact too. */
+
+static int half_quantum(double ax)            /* exponent of the binary16 ulp at |x| = ax > 0 */
+{
+    const int e = ilogb(ax);
+    return e >= -14 ? e - 10 : -24;
+}
+
+double wo_half_round(double x)
+{
+    if (isnan(x) || x == 0.0) return x;
+    const double ax = fabs(x);
+    if (ax >= 65520.0) return copysign(INFINITY, x);   /* past the largest finite value's tie */
+    const int q = half_quantum(ax);
+    return copysign(ldexp(nearbyint(ldexp(ax, -q)), q), x);   /* default mode: ties to even */
+}
+
+double wo_half_fma_relu(double a, double b, double c)
+{
+    const double p = a * b;                   /* exact: two 11-bit significands */
+    const double s = p + c;
+    const double bb = s - p;
+    const double err = (p - (s - bb)) + (c - bb);   /* s + err == p + c exactly */
+    double r = wo_half_round(s);
+    if (err != 0.0 && isfinite(s)) {
+        /* only a value of s exactly on a binary16 tie can round the wrong way:
+         * the exact sum lies past the tie on err's side */
+        const double as = fabs(s);
+        const int q = half_quantum(as < 65504.0 ? as : 65504.0);
+        const double sc = ldexp(as, -q), fl = floor(sc);
+        if (sc - fl == 0.5) {
+            const double mag = ((err > 0) == (s > 0)) ? fl + 1.0 : fl;
+            r = copysign(ldexp(mag, q), s);
+            if (fabs(r) > 65504.0) r = copysign(INFINITY, s);
+        }
+    }
+    return r < 0.0 ? 0.0 : r;
+}
+
+static unsigned learned16_one(const wo_code_t* c, int T, int cap, const float* Ah, const float* NBh,
+                              const float* llr, float* P, int8_t* out, float* msg, int32_t* iters,
+                              int32_t* synfail)
+{
+    const int z = c->z, n = c->n;
+    for (int v = 0; v < n; v++) {
+        const float x = fminf(fmaxf(llr[v], -2048.0f), 2048.0f);
+        const double h = wo_half_round((double)x);
+        P[v] = h == 0.0 ? 0.0f : (float)h;    /* -0 becomes +0 */
+    }
+    slice(P, out, n);
+    if (syndrome_one(c, out, 1) == 0) {
+        if (iters) *iters = 0;
+        if (synfail) *synfail = 0;
+        return 0;
+    }
+    memset(msg, 0, sizeof(float) * (size_t)c->nblk * z);
+    for (int it = 0; it < cap; it++) {
+        const int t = it < T ? it : T - 1;
+        for (int i = 0; i < c->mb; i++) {
+            const int b0 = c->row_start[i], d = c->row_start[i + 1] - b0;
+            for (int r = 0; r < z; r++) {
+                float L[WO_NB];
+                int v[WO_NB];
+                unsigned negpar = 0;
+                float m1 = INFINITY, m2 = INFINITY;
+                for (int e = 0; e < d; e++) {
+                    v[e] = var_of(c, b0 + e, r);
+                    L[e] = (float)wo_half_round((double)P[v[e]] - (double)msg[(b0 + e) * z + r]);
+                    negpar ^= (unsigned)(signbit(L[e]) != 0);
+                    const float a = fabsf(L[e]);
+                    m2 = fminf(m2, fmaxf(m1, a));
+                    m1 = fminf(m1, a);
+                }
+                m1 = fminf(m1, 2048.0f);
+                m2 = fminf(m2, 2048.0f);
+                for (int e = 0; e < d; e++) {
+                    const unsigned neg = negpar ^ (unsigned)(signbit(L[e]) != 0) ^ (unsigned)(d & 1);
+                    const float mu = (fabsf(L[e]) == m1) ? m2 : m1;
+                    const size_t wi = widx(t, i, c->blk_col[b0 + e]);
+                    const float mag = (float)wo_half_fma_relu((double)Ah[wi], (double)mu, (double)NBh[wi]);
+                    const float m = flip_sign(mag, neg);
+                    msg[(b0 + e) * z + r] = m;
+                    P[v[e]] = (float)wo_half_round((double)L[e] + (double)m);
+                }
+            }
+        }
+        slice(P, out, n);
+        if (syndrome_one(c, out, 1) == 0) {
+            if (iters) *iters = it + 1;
+            if (synfail) *synfail = 0;
+            return 0;
+        }
+    }
+    if (iters) *iters = cap;
+    if (synfail) *synfail = 1;
+    return 1;
+}
+
+int wo_learned16_decode_batch(int rate, int z, int iterations, int cap, const float* w, long frames,
+                              const float* llr, float* post, int8_t* decoded, int32_t* iters, int32_t* synfail,
+                              int threads)
+{
+    wo_code_t c;
+    if (wo_code(rate, z, &c)) return -1;
+    if (iterations < 1 || iterations > 8 || cap < 0) return -1;
+    const size_t WN = (size_t)iterations * WO_L * WO_NB;
+    float* Ah = (float*)malloc(sizeof(float) * 2 * WN);
+    if (!Ah) return -1;
+    float* NBh = Ah + WN;
+    for (size_t j = 0; j < WN; j++) {
+        Ah[j] = (float)wo_half_round((double)w[j]);
+        NBh[j] = (float)wo_half_round(-(double)w[WN + j]);
+    }
+    if (threads < 1) threads = 1;
+    #pragma omp parallel num_threads(threads)
+    {
+        float* msg = (float*)malloc(sizeof(float) * (size_t)c.nblk * z);
+        #pragma omp for schedule(dynamic, 16)
+        for (long f = 0; f < frames; f++)
+            learned16_one(&c, iterations, cap, Ah, NBh, llr + f * c.n, post + f * c.n, decoded + f * c.n, msg,
+                          iters ? iters + f : NULL, synfail ? synfail + f : NULL);
+        free(msg);
+    }
+    free(Ah);
+    return 0;
+}
+
 /* log(1 + exp(x)) and the logistic function, both stable for large |x|. */
 static double softplus(double x) { return x > 0 ? x + log1p(exp(-x)) : log1p(exp(x)); }
 static double sigmoid(double x) { return x >= 0 ? 1.0 / (1.0 + exp(-x)) : exp(x) / (1.0 + exp(x)); }

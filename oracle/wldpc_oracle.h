@@ -92,6 +92,19 @@ int wo_framegen(int rate, int z, uint64_t seed, uint64_t first_frame, long frame
 int wo_learned_decode_batch(int rate, int z, int iterations, int cap, const float* w, long frames,
                             float* llr, int8_t* decoded, int32_t* iters, int32_t* synfail,
                             int threads);
+/* Learned min-sum in binary16, as the packed-half decoder computes it (one
+ * frame at a time; the device's lanes are independent): LLRs clamped to
+ * +-2048 and rounded to binary16 (-0 made +0), weights rounded to binary16,
+ * every difference, sum and fused multiply-add rounded once to binary16
+ * (nearest even), row minima clamped to 2048; post receives the posteriors
+ * (binary16 values as floats); llr is not modified. */
+int wo_learned16_decode_batch(int rate, int z, int iterations, int cap, const float* w, long frames,
+                              const float* llr, float* post, int8_t* decoded, int32_t* iters, int32_t* synfail,
+                              int threads);
+/* x rounded to the nearest binary16 value (ties to even, overflow to inf),
+ * and relu of a*b + c rounded once to binary16. */
+double wo_half_round(double x);
+double wo_half_fma_relu(double a, double b, double c);
 /* Learned min-sum training step reference in double precision: loss
  * (mean BCE over iterations, frames and bits, positive LLR = bit 1) and its
  * gradient with respect to w (same layout as above). */

@@ -22,6 +22,7 @@ HALFRATE, TWOTHIRDSA, TWOTHIRDSB, THREEQUARTERSA, THREEQUARTERSB, FIVESIXTHS = r
 RATE_NAMES = ["1/2", "2/3A", "2/3B", "3/4A", "3/4B", "5/6"]
 Z_VALUES = tuple(range(24, 97, 4))
 MODE_NMS, MODE_OMS, MODE_MS = 0, 1, 2
+LMS_F32, LMS_F16X2 = 0, 1   # learned-decoder inference arithmetic (wldpc_lms_set_precision)
 
 OK = 0
 ERR_ARG, ERR_CODE, ERR_CUDA, ERR_NO_DEVICE, ERR_TIMEOUT, ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6
@@ -85,6 +86,7 @@ def _lib():
     L.wldpc_lms_get_weights.argtypes = [_p, _p]
     L.wldpc_lms_decode_device.argtypes = [_p, _p, _p, _p, _p, _sz, _p]
     L.wldpc_lms_set_cap.argtypes = [_p, _u]
+    L.wldpc_lms_set_precision.argtypes = [_p, _i]
     L.wldpc_lms_decode_host.argtypes = [_p, _p, _p, _p, _p, _sz]
     L.wldpc_lms_loss_grad.argtypes = [_p, _p, _p, _sz, _p, ctypes.POINTER(ctypes.c_double)]
     L.wldpc_lms_train.argtypes = [_p, _u, _u, ctypes.c_float, ctypes.c_float, ctypes.c_uint64, ctypes.c_uint64,
@@ -340,17 +342,27 @@ class LearnedDecoder:
     """wldpc_lms handle: learned normalized/offset min-sum (weights per
     iteration, layer and base column), its training and inference."""
 
-    def __init__(self, rate: int, z: int, iterations: int = 8, weights=None, cap: int | None = None):
+    def __init__(self, rate: int, z: int, iterations: int = 8, weights=None, cap: int | None = None,
+                 precision: int = LMS_F32):
         self.rate, self.z, self.iterations = rate, z, iterations
         self.info = code_info(rate, z)
         self.n, self.k = self.info.n, self.info.k
         h = ctypes.c_void_p()
         _check(_lib().wldpc_lms_create(rate, z, iterations, ctypes.byref(h)), "learned decoder")
         self._h = h
+        self.precision = LMS_F32
         if weights is not None:
             self.set_weights(weights)
         if cap is not None:
             self.set_cap(cap)
+        if precision != LMS_F32:
+            self.set_precision(precision)
+
+    def set_precision(self, precision: int) -> None:
+        """LMS_F32 (fp32 inference) or LMS_F16X2 (two frames per thread in
+        packed binary16; needs |a| <= 2 and |b| <= 1024)."""
+        _check(_lib().wldpc_lms_set_precision(self._h, precision), "set_precision")
+        self.precision = precision
 
     def set_cap(self, cap: int) -> None:
         """Iteration cap; iterations past the trained ones reuse the last iteration's weights."""

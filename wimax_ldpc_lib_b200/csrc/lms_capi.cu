@@ -10,6 +10,7 @@
 #include <cstring>
 #include <new>
 #include <vector>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "wimax_ldpc_b200.h"
@@ -101,6 +102,7 @@ inline bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_
 struct wldpc_lms {
     int rate, z, T, nblk;
     int cap;                 /* decoding iteration cap (>= 1); iterations past T reuse row T-1 */
+    int precision = WLDPC_LMS_F32;   /* inference arithmetic (training is always fp32) */
     CodeDesc code;
     const LmsLaunch* k;
     LmsWeights w;            /* host copy, compact [T][nblk], used by inference launches */
@@ -236,11 +238,51 @@ int wldpc_lms_get_weights(wldpc_lms* h, float* table)
     return WLDPC_OK;
 }
 
+/* the packed-half decoder accepts |a| <= 2 and |b| <= 1024, which keeps every
+ * binary16 sum of the decode finite (lms16.cuh) */
+static bool lms16_weights_ok(const wldpc_lms* h)
+{
+    for (int t = 0; t < h->T; t++)
+        for (int b = 0; b < h->nblk; b++)
+            if (!(fabsf(h->w.a[t][b]) <= kLms16MaxScale) || !(fabsf(h->w.b[t][b]) <= kLms16MaxOffset)) return false;
+    return true;
+}
+
+static uint32_t half_pair_bits(float x)
+{
+    const __half v = __float2half_rn(x);
+    const uint32_t u = __half_as_ushort(v);
+    return u | (u << 16);
+}
+
+static int lms16_launch_decode(wldpc_lms* h, const float* llr, int8_t* hard, float* post, int32_t* status,
+                               size_t frames, cudaStream_t st)
+{
+    if (!lms16_weights_ok(h)) return WLDPC_ERR_ARG;
+    Lms16Args a;
+    a.llr = llr;
+    a.hard = hard;
+    a.post = post;
+    a.status = status;
+    a.frames = (long long)frames;
+    a.iters = h->cap;
+    a.wrows = h->T;
+    for (int t = 0; t < h->T; t++)
+        for (int b = 0; b < h->nblk; b++)
+            a.wab[t][b] = make_uint2(half_pair_bits(h->w.a[t][b]), half_pair_bits(-h->w.b[t][b]));
+    const LmsLaunch* k = h->k;
+    const long long ctas = ((long long)frames + k->frames16 - 1) / k->frames16;
+    k->decode16<<<(unsigned)ctas, k->threads16, 0, st>>>(a);
+    CU(cudaGetLastError());
+    return WLDPC_OK;
+}
+
 static int lms_launch_decode(wldpc_lms* h, const float* llr, int8_t* hard, float* post, int32_t* status,
                              size_t frames, cudaStream_t st)
 {
     int rc = lms_sync_host_weights(h);
     if (rc) return rc;
+    if (h->precision == WLDPC_LMS_F16X2) return lms16_launch_decode(h, llr, hard, post, status, frames, st);
     LmsArgs a;
     a.llr = llr;
     a.hard = hard;
@@ -269,6 +311,18 @@ int wldpc_lms_decode_device(wldpc_lms* h, const float* llr, int8_t* decoded, flo
         return WLDPC_ERR_ARG;
     if (frames == 0) return WLDPC_OK;
     return lms_launch_decode(h, llr, decoded, posterior, status, frames, (cudaStream_t)stream);
+}
+
+int wldpc_lms_set_precision(wldpc_lms* h, int precision)
+{
+    if (!h || (precision != WLDPC_LMS_F32 && precision != WLDPC_LMS_F16X2)) return WLDPC_ERR_ARG;
+    if (precision == WLDPC_LMS_F16X2) {
+        int rc = lms_sync_host_weights(h);
+        if (rc) return rc;
+        if (!lms16_weights_ok(h)) return WLDPC_ERR_ARG;
+    }
+    h->precision = precision;
+    return WLDPC_OK;
 }
 
 int wldpc_lms_set_cap(wldpc_lms* h, unsigned cap)

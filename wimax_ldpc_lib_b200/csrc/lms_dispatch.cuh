@@ -1,8 +1,9 @@
-/* Dispatch table of the learned min-sum kernels (lms.cuh). */
+/* Dispatch table of the learned min-sum kernels (lms.cuh, lms16.cuh). */
 #ifndef WLDPC_LMS_DISPATCH_CUH
 #define WLDPC_LMS_DISPATCH_CUH
 
 #include "lms.cuh"
+#include "lms16.cuh"
 
 namespace wldpc {
 
@@ -14,6 +15,8 @@ struct LmsLaunch {
     int threads, frames_per_cta, smem;
     void (*train)(const LmsTrainArgs);
     int train_smem;          /* train CTA = z threads, one frame */
+    void (*decode16)(const Lms16Args);   /* packed-half decoder (lms16.cuh) */
+    int threads16, frames16;             /* its CTA size and frames per CTA (static shared memory) */
 };
 
 const LmsLaunch* lms_entry(int rate, int z);
