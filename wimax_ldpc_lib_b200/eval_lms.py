@@ -7,7 +7,9 @@ For every Eb/N0 point (default 1.0 to 3.0 dB in 0.25 dB steps) it generates
 held-out frames on the device (a seed and frame counters disjoint from
 training), decodes the same frames with the learned decoder at its trained cap T and at
 the reference's cap 10 (iterations past T reuse the last trained weights),
-and with the plain normalized min-sum at caps T and 10, and records FER, info
+the learned decoder in packed binary16 at cap 10 (`learned10_f16x2`, where the
+weights are in its range), and with the plain normalized min-sum at caps T and
+10, and records FER, info
 BER, mean iterations and kernel-only info Gbit/s (CUDA events). The learned
 weights ship at a point and cap when their frame errors on those frames are
 no more than the plain decoder's at the same cap and they need fewer
@@ -45,6 +47,8 @@ def evaluate(meta, frames=1 << 20, batch=1 << 18, points=None, log=print):
     decs = {"learned": wl.LearnedDecoder(rate, z, T, weights=w),
             "learned10": wl.LearnedDecoder(rate, z, T, weights=w, cap=10),
             f"plain{T}": wl.Decoder(rate, z, T), "plain10": wl.Decoder(rate, z, 10)}
+    if np.abs(w[0]).max() <= 2.0 and np.abs(w[1]).max() <= 1024.0:
+        decs["learned10_f16x2"] = wl.LearnedDecoder(rate, z, T, weights=w, cap=10, precision=wl.LMS_F16X2)
     llr = torch.empty((batch, n), dtype=torch.float32, device="cuda")
     info = torch.empty((batch, kk), dtype=torch.uint8, device="cuda")
     hard = torch.empty((batch, n), dtype=torch.int8, device="cuda")
@@ -85,12 +89,20 @@ def evaluate(meta, frames=1 << 20, batch=1 << 18, points=None, log=print):
                                  L10["mean_iterations"] < P["mean_iterations"])
         row[f"ship_cap{T}"] = bool(L["frame_errors"] <= P8["frame_errors"] and
                                    L["mean_iterations"] < P8["mean_iterations"])
+        if "learned10_f16x2" in row:
+            H = row["learned10_f16x2"]
+            row["ship_cap10_f16x2"] = bool(H["frame_errors"] <= P["frame_errors"] and
+                                           H["mean_iterations"] < P["mean_iterations"])
         rows.append(row)
         log(f"{eb:5.2f} dB | learned{T} FER {L['fer']:.2e} it {L['mean_iterations']:.2f} {L['info_gbps']:.1f} Gb/s "
             f"| plain{T} FER {P8['fer']:.2e} it {P8['mean_iterations']:.2f} | learned10 FER {L10['fer']:.2e} "
             f"it {L10['mean_iterations']:.2f} {L10['info_gbps']:.1f} Gb/s | plain10 FER {P['fer']:.2e} "
             f"it {P['mean_iterations']:.2f} {P['info_gbps']:.1f} Gb/s | ship@10 {row['ship_cap10']} "
             f"ship@{T} {row[f'ship_cap{T}']}")
+        if "learned10_f16x2" in row:
+            H = row["learned10_f16x2"]
+            log(f"{'':5s}    | learned10 f16x2 FER {H['fer']:.2e} it {H['mean_iterations']:.2f} "
+                f"{H['info_gbps']:.1f} Gb/s | ship@10 {row['ship_cap10_f16x2']}")
     return rows
 
 
@@ -99,6 +111,8 @@ def main():
     ap.add_argument("weights")
     ap.add_argument("--frames", type=int, default=1 << 20)
     ap.add_argument("--points", type=float, nargs="*", default=None)
+    ap.add_argument("--out", default=None, help="where to write the weight file with its evaluation "
+                                                "(default: in place)")
     args = ap.parse_args()
     with open(args.weights) as f:
         meta = json.load(f)
@@ -106,11 +120,13 @@ def main():
     import torch
     meta["evaluation"] = {"seed": EVAL_SEED, "frames_per_point": args.frames, "device": torch.cuda.get_device_name(0),
                           "rule": "ship at a cap where learned frame errors <= plain frame errors at that cap on "
-                                  "the same held-out frames and learned mean iterations < plain mean iterations",
+                                  "the same held-out frames and learned mean iterations < plain mean iterations "
+                                  "(fp32 and, at cap 10, packed binary16)",
                           "points": rows}
-    with open(args.weights, "w") as f:
+    out = args.out or args.weights
+    with open(out, "w") as f:
         json.dump(meta, f)
-    print(f"evaluation written into {args.weights}")
+    print(f"evaluation written into {out}")
 
 
 if __name__ == "__main__":
