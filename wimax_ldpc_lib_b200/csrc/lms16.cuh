@@ -57,7 +57,6 @@ namespace wldpc {
 constexpr float kLms16Clamp = 2048.0f;          /* input LLR and min-magnitude bound */
 constexpr uint32_t kH2Clamp = 0x68006800u;      /* (2048, 2048) in binary16 */
 constexpr uint32_t kH2Sign = 0x80008000u;
-constexpr uint32_t kH2Abs = 0x7fff7fffu;
 constexpr float kLms16MaxScale = 2.0f;          /* accepted |a| */
 constexpr float kLms16MaxOffset = 1024.0f;      /* accepted |b| */
 
@@ -124,6 +123,14 @@ __device__ __forceinline__ uint32_t h2_eq_mask(uint32_t a, uint32_t b)
 {
     uint32_t d;
     asm("set.eq.u32.f16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+/* |a| per lane (an f16x2 abs, which the compiler can fold into the consuming
+ * min/max/set as an operand modifier; an integer AND cannot be folded) */
+__device__ __forceinline__ uint32_t h2_abs(uint32_t a)
+{
+    uint32_t d;
+    asm("abs.f16x2 %0, %1;" : "=r"(d) : "r"(a));
     return d;
 }
 /* two floats -> f16x2 (round to nearest even), lane 0 = lo */
@@ -278,7 +285,7 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
                     constexpr int e = decltype(E_)::value;
                     X[e] = P[edge_var_c<R, Z, I, e>(r)];
                     L[e] = h2_sub(X[e], Mr[b0 + e]);
-                    A[e] = L[e] & kH2Abs;
+                    A[e] = h2_abs(L[e]);
                     sgn ^= L[e];
                 });
                 uint32_t m1, m2;
