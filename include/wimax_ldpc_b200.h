@@ -213,8 +213,9 @@ WLDPC_API int wldpc_lms_set_cap(wldpc_lms* h, unsigned cap);
  * rounds to binary16, input LLRs are clamped to +-2048 and row minima to
  * 2048, weights are rounded to binary16, and the posteriors returned are the
  * exact float values of the binary16 results. A frame's outputs do not depend
- * on the other frames of the batch. F16X2 needs |a| <= 2 and |b| <= 1024 for
- * every weight, which keeps every sum finite; otherwise this call, or a
+ * on the other frames of the batch. F16X2 needs |a| <= 2 and 0 <= b <= 1024
+ * for every weight (finite sums; zero messages for a stopped frame whose
+ * partner decodes on); otherwise this call, or a
  * decode after training moved a weight out of range, returns WLDPC_ERR_ARG.
  * Training always runs in fp32. */
 #define WLDPC_LMS_F32 0

@@ -11,10 +11,17 @@ import numpy as np
 import pytest
 
 import inputs
-from test_learned_oracle import random_weights
+from test_learned_oracle import random_weights as random_weights_any
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def random_weights(oracle, rate, z, T, seed):
+    """random weights in the packed-half decoder's range (offsets b >= 0)"""
+    w, rs, cols = random_weights_any(oracle, rate, z, T, seed)
+    w[1] = np.abs(w[1])
+    return w, rs, cols
 
 
 def check_equal(out, ref):
@@ -92,6 +99,11 @@ def test_learned16_rejects_out_of_range_weights(wl, cuda, oracle):
     lms2 = wl.LearnedDecoder(rate, z, T, weights=bad)
     with pytest.raises(wl.LdpcError):
         lms2.set_precision(wl.LMS_F16X2)
+    neg = w.copy()
+    neg[1, 1, 2, cols[rs[2]]] = -0.01          # offsets must be >= 0
+    lms3 = wl.LearnedDecoder(rate, z, T, weights=neg)
+    with pytest.raises(wl.LdpcError):
+        lms3.set_precision(wl.LMS_F16X2)
     with pytest.raises(wl.LdpcError):
         lms2.set_precision(7)
 

@@ -360,7 +360,7 @@ class LearnedDecoder:
 
     def set_precision(self, precision: int) -> None:
         """LMS_F32 (fp32 inference) or LMS_F16X2 (two frames per thread in
-        packed binary16; needs |a| <= 2 and |b| <= 1024)."""
+        packed binary16; needs |a| <= 2 and 0 <= b <= 1024)."""
         _check(_lib().wldpc_lms_set_precision(self._h, precision), "set_precision")
         self.precision = precision
 

@@ -23,17 +23,20 @@
  * with h() rounding to binary16 and s_e the sign the other edges imply
  * (positive LLR = bit 1, so an odd-degree row flips the product of the other
  * signs). Bounds: |llr| <= 2048 and mu <= 2048, and the host accepts only
- * |a| <= 2 and |b| <= 1024, so |m'| <= 5120 and, with at most 6 edges per
+ * |a| <= 2 and 0 <= b <= 1024, so |m'| <= 4096 and, with at most 6 edges per
  * variable, every posterior stays below 32768: no value overflows. A -0
  * never appears after staging (x - y and x + y give -0 only from a -0
  * operand), so the sign bit of a posterior is its hard decision (x >= 0 is
  * bit 1) and a row's parity is an XOR of sign bits.
  *
  * Early exit per frame: after staging and after every iteration each frame's
- * syndrome is checked; a frame whose syndrome is zero is frozen (its lane's
- * posteriors are kept by a bitwise select while its partner decodes on) and
- * its iteration count stops. The CTA runs while any of its frames is
- * decoding.
+ * syndrome is checked; a frame whose syndrome is zero is frozen and its
+ * iteration count stops, while its partner decodes on. A frozen lane's
+ * messages are set to +0 once and its row minima are masked to 0 in every
+ * later layer, so its new messages are s * relu(a*0 - b) = +-0 (b >= 0) and
+ * its posteriors are recomputed as (P - 0) + (+-0) = P exactly: they stay as
+ * they were when the frame stopped, with no per-edge select. The CTA runs
+ * while any of its frames is decoding.
  *
  * Mapping: GP = 32/gcd(z, 32) frame pairs per CTA, so that GP*z threads fill
  * whole warps (z = 96: one pair of 96 threads; z = 48: two pairs; z = 24:
@@ -58,7 +61,7 @@ constexpr float kLms16Clamp = 2048.0f;          /* input LLR and min-magnitude b
 constexpr uint32_t kH2Clamp = 0x68006800u;      /* (2048, 2048) in binary16 */
 constexpr uint32_t kH2Sign = 0x80008000u;
 constexpr float kLms16MaxScale = 2.0f;          /* accepted |a| */
-constexpr float kLms16MaxOffset = 1024.0f;      /* accepted |b| */
+constexpr float kLms16MaxOffset = 1024.0f;      /* accepted b, which must also be >= 0 */
 
 struct Lms16Args {
     const float* llr;       /* frames x n, 16-byte aligned */
@@ -273,25 +276,24 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
 
     for (int t = 0; t < a.iters && fmask != 0u; ++t) {
         if (tid == 0) s_fail[(t + 1) & 1] = 0;
-        const uint32_t keep = ~h2_lanes(act);  /* frozen lanes keep their posteriors */
+        const uint32_t am = h2_lanes(act);     /* lanes still decoding; frozen lanes get mu = 0 */
         const uint2* wab = a.wab[t < a.wrows ? t : a.wrows - 1];
         static_for<MB>([&](auto I) {
             constexpr int d = layer_degree(R, I);
             constexpr int b0 = block_index(R, I, 0);
             if (act) {
-                uint32_t X[d], L[d], A[d];
+                uint32_t L[d], A[d];
                 uint32_t sgn = 0;
                 static_for<d>([&](auto E_) {
                     constexpr int e = decltype(E_)::value;
-                    X[e] = P[edge_var_c<R, Z, I, e>(r)];
-                    L[e] = h2_sub(X[e], Mr[b0 + e]);
+                    L[e] = h2_sub(P[edge_var_c<R, Z, I, e>(r)], Mr[b0 + e]);
                     A[e] = h2_abs(L[e]);
                     sgn ^= L[e];
                 });
                 uint32_t m1, m2;
                 two_min_h2<0, d>(A, m1, m2);
-                m1 = h2_min(m1, kH2Clamp);
-                m2 = h2_min(m2, kH2Clamp);
+                m1 = h2_min(m1, kH2Clamp) & am;
+                m2 = h2_min(m2, kH2Clamp) & am;
                 /* positive LLR = bit 1: the extrinsic sign flips on odd-degree rows */
                 const uint32_t fb = (sgn ^ ((d & 1) ? kH2Sign : 0u)) & kH2Sign;
                 static_for<d>([&](auto E_) {
@@ -303,7 +305,7 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
                     const uint32_t msg = mag | ((L[e] ^ fb) & kH2Sign);
                     Mr[b0 + e] = msg;
                     const uint32_t pn = h2_add(L[e], msg);
-                    P[edge_var_c<R, Z, I, e>(r)] = (pn & ~keep) | (X[e] & keep);
+                    P[edge_var_c<R, Z, I, e>(r)] = pn;
                 });
             }
             __syncthreads();
@@ -311,7 +313,13 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
         fmask = frame_fail(act ? rows_fail() & h2_lanes(act) : 0u, (t + 1) & 1);
         if (act & 1u) it0 = t + 1;
         if (act & 2u) it1 = t + 1;
-        act = (fmask >> (2 * g)) & 3u;
+        const unsigned nact = (fmask >> (2 * g)) & 3u;
+        if (act & ~nact) {   /* lanes that stopped now: their messages become +0 */
+            const uint32_t drop = ~h2_lanes(act & ~nact);
+#pragma unroll
+            for (int q = 0; q < S::NBLK; q++) Mr[q] &= drop;
+        }
+        act = nact;
     }
 
     /* outputs: hard bits (sign clear = bit 1) and the posteriors as floats */

@@ -238,13 +238,15 @@ int wldpc_lms_get_weights(wldpc_lms* h, float* table)
     return WLDPC_OK;
 }
 
-/* the packed-half decoder accepts |a| <= 2 and |b| <= 1024, which keeps every
- * binary16 sum of the decode finite (lms16.cuh) */
+/* the packed-half decoder accepts |a| <= 2 and 0 <= b <= 1024: the bounds keep
+ * every binary16 sum of the decode finite, and b >= 0 is what lets a stopped
+ * frame's lane produce zero messages (lms16.cuh) */
 static bool lms16_weights_ok(const wldpc_lms* h)
 {
     for (int t = 0; t < h->T; t++)
         for (int b = 0; b < h->nblk; b++)
-            if (!(fabsf(h->w.a[t][b]) <= kLms16MaxScale) || !(fabsf(h->w.b[t][b]) <= kLms16MaxOffset)) return false;
+            if (!(fabsf(h->w.a[t][b]) <= kLms16MaxScale) || !(h->w.b[t][b] >= 0.0f && h->w.b[t][b] <= kLms16MaxOffset))
+                return false;
     return true;
 }
 

@@ -47,7 +47,7 @@ def evaluate(meta, frames=1 << 20, batch=1 << 18, points=None, log=print):
     decs = {"learned": wl.LearnedDecoder(rate, z, T, weights=w),
             "learned10": wl.LearnedDecoder(rate, z, T, weights=w, cap=10),
             f"plain{T}": wl.Decoder(rate, z, T), "plain10": wl.Decoder(rate, z, 10)}
-    if np.abs(w[0]).max() <= 2.0 and np.abs(w[1]).max() <= 1024.0:
+    if np.abs(w[0]).max() <= 2.0 and w[1].min() >= 0.0 and w[1].max() <= 1024.0:
         decs["learned10_f16x2"] = wl.LearnedDecoder(rate, z, T, weights=w, cap=10, precision=wl.LMS_F16X2)
     llr = torch.empty((batch, n), dtype=torch.float32, device="cuda")
     info = torch.empty((batch, kk), dtype=torch.uint8, device="cuda")
