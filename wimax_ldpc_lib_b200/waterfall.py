@@ -7,8 +7,8 @@ Writes the JSON result and the same points as CSV beside it (results/waterfall.c
 Frames are generated, encoded, modulated, corrupted and decoded on the
 device (framegen, or null-space codewords for 3/4B, which has no
 dual-diagonal encoder). For every (rate, z) and decoder (plain normalized
-min-sum, cap 10; the learned min-sum, cap 10, where trained weights for that
-code are shipped) the Eb/N0 sweep starts at --start dB and steps by 0.1 dB;
+min-sum, cap 10; the learned min-sum, cap 10, in fp32 and in packed binary16,
+where trained weights for that code are shipped) the Eb/N0 sweep starts at --start dB and steps by 0.1 dB;
 each point runs batches until at least 200 information-bit errors (or a bit
 budget) and the sweep stops once BER < 1e-6. Reported per point: FER, info
 BER, the reference BER_runner's BER (codeword-bit errors over info bits,
@@ -232,8 +232,11 @@ def main():
             decs = {"plain": wl.Decoder(rate, z, 10)}
             meta = learned_weights(rate, z)
             if meta is not None:
-                decs["learned"] = wl.LearnedDecoder(rate, z, meta["iterations"],
-                                                    weights=np.array(meta["weights"], np.float32), cap=10)
+                w = np.array(meta["weights"], np.float32)
+                decs["learned"] = wl.LearnedDecoder(rate, z, meta["iterations"], weights=w, cap=10)
+                if np.abs(w[0]).max() <= 2.0 and w[1].min() >= 0.0 and w[1].max() <= 1024.0:
+                    decs["learned_f16x2"] = wl.LearnedDecoder(rate, z, meta["iterations"], weights=w, cap=10,
+                                                              precision=wl.LMS_F16X2)
             for name, dec in decs.items():
                 print(f"{RATE_NAMES[rate]} z={z} {name}")
                 pts = sweep(rate, z, dec, start=args.start if args.start is not None else starts[rate],
