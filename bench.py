@@ -16,9 +16,10 @@ plain one's; `decoders` reports all three.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
   value      kernel-only info Gbit/s, LLRs resident in HBM
-  e2e        the same metric through the C ABI host call
-             (wldpc_decode_batch_host: copy-in, decode, posterior + hard bits
-             copied back, as the reference's decode(float*) returns them)
+  e2e        the same metric through the C ABI host call of the headline
+             decoder (wldpc_lms_decode_host, or wldpc_decode_batch_host for
+             the plain one: copy-in, decode, posterior + hard bits copied
+             back, as the reference's decode(float*) returns them)
   roofline   the decode kernel against the measured HBM copy bandwidth
   cpu_baseline  the reference's own OpenMP decoder (compiled from its sources)
              on this machine's host cores, on a bounded sample of the workload
