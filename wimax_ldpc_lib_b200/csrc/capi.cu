@@ -116,7 +116,7 @@ const char* wldpc_strerror(int code)
     }
 }
 
-int wldpc_version(void) { return 10000; }
+int wldpc_version(void) { return 10100; }   /* 1.1.0: wldpc_lms_set_precision */
 
 int wldpc_code_info_get(int rate, unsigned z, wldpc_code_info* out)
 {
