@@ -213,6 +213,14 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
     const long long left = a.frames - f0;
     const int nf = left < FR ? (int)left : FR;
     uint32_t* P = sP + g * N;
+    /* edge (I, E) of row r lives at col*Z + (r + s) mod Z: with the two bases
+     * P + r and P + r - Z that is one compare and one select per edge, the
+     * constant col*Z + s folding into the shared-memory access */
+    float* const Pr = reinterpret_cast<float*>(P) + r;
+    float* const Prz = Pr - Z;
+    auto at = [&](auto I, auto E) -> uint32_t* {
+        return reinterpret_cast<uint32_t*>(edge_ptr<R, Z, decltype(I)::value, decltype(E)::value>(Pr, Prz, r));
+    };
 
     if (tid == 0) {
         s_fail[0] = 0;
@@ -251,7 +259,7 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
         static_for<MB>([&](auto I) {
             constexpr int d = layer_degree(R, I);
             uint32_t x = (d & 1) ? kH2Sign : 0u;   /* parity of the hard bits: d minus the negatives */
-            static_for<d>([&](auto E_) { x ^= P[edge_var_c<R, Z, I, E_>(r)]; });
+            static_for<d>([&](auto E_) { x ^= *at(I, E_); });
             acc |= x;
         });
         return acc & kH2Sign;
@@ -286,7 +294,7 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
                 uint32_t sgn = 0;
                 static_for<d>([&](auto E_) {
                     constexpr int e = decltype(E_)::value;
-                    L[e] = h2_sub(P[edge_var_c<R, Z, I, e>(r)], Mr[b0 + e]);
+                    L[e] = h2_sub(*at(I, E_), Mr[b0 + e]);
                     A[e] = h2_abs(L[e]);
                     sgn ^= L[e];
                 });
@@ -305,7 +313,7 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
                     const uint32_t msg = mag | ((L[e] ^ fb) & kH2Sign);
                     Mr[b0 + e] = msg;
                     const uint32_t pn = h2_add(L[e], msg);
-                    P[edge_var_c<R, Z, I, e>(r)] = pn;
+                    *at(I, E_) = pn;
                 });
             }
             __syncthreads();
