@@ -249,7 +249,7 @@ def run_ours(args):
         with open(LMS_WEIGHTS) as f:
             lms_meta = json.load(f)
         # the learned decoder at the reference's cap (iterations past the trained
-        # ones reuse the last trained weights), judged against plain at cap 10
+        # ones reuse the last trained weights), compared with plain at cap 10
         decoders["learned"] = wl.LearnedDecoder(RATE, Z, lms_meta["iterations"],
                                                 weights=np.array(lms_meta["weights"], np.float32), cap=MAX_ITER)
         # the same network decoded in packed binary16, two frames per thread

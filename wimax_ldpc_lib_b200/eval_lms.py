@@ -13,7 +13,7 @@ weights are in its range), and with the plain normalized min-sum at caps T and
 BER, mean iterations and kernel-only info Gbit/s (CUDA events). The learned
 weights ship at a point and cap when their frame errors on those frames are
 no more than the plain decoder's at the same cap and they need fewer
-iterations on average (plain min-sum stays the judge and the fallback). The
+iterations on average (plain min-sum stays the yardstick and the fallback). The
 table is written back into the weight file under "evaluation".
 """
 from __future__ import annotations
