@@ -108,6 +108,7 @@ def test_argument_checks_of_the_additions(wl):
     assert L.wldpc_lms_grad_size(None, ctypes.byref(nw)) == wl.ERR_ARG
     assert L.wldpc_lms_step_grad(None, 16, 1.0, 2.0, 1, 0, None, None, None) == wl.ERR_ARG
     assert L.wldpc_lms_apply_grad(None, None, 1e-3, None) == wl.ERR_ARG
+    assert L.wldpc_lms_set_precision(None, wl.LMS_F16X2) == wl.ERR_ARG
     # mixed batch: variant numbering rate * 19 + (z - 24) / 4, bad codes, bad caps
     assert L.wldpc_variant(0, 24) == 0 and L.wldpc_variant(0, 96) == 18 and L.wldpc_variant(5, 96) == 113
     assert L.wldpc_variant(6, 96) == wl.ERR_CODE and L.wldpc_variant(0, 26) == wl.ERR_CODE
