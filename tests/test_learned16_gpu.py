@@ -33,8 +33,13 @@ def check_equal(out, ref):
     assert (((st >> 16) & 1) == so).all(), "syndrome flag"
 
 
-@pytest.mark.parametrize("rate,z,frames", [(0, 96, 257), (0, 48, 131), (0, 24, 203), (1, 96, 64),
-                                           (2, 48, 75), (3, 24, 97), (4, 96, 33), (5, 48, 129)])
+# every code the learned decoder supports (6 rates x z = 24, 48, 96), odd and even batch sizes
+CODES16 = [(0, 96, 257), (0, 48, 131), (0, 24, 203), (1, 96, 64), (1, 48, 41), (1, 24, 66), (2, 96, 39),
+           (2, 48, 75), (2, 24, 50), (3, 96, 45), (3, 48, 52), (3, 24, 97), (4, 96, 33), (4, 48, 70),
+           (4, 24, 81), (5, 96, 36), (5, 48, 129), (5, 24, 58)]
+
+
+@pytest.mark.parametrize("rate,z,frames", CODES16)
 def test_learned16_decode_matches_oracle(wl, cuda, oracle, rate, z, frames):
     T = 8
     w, _, _ = random_weights(oracle, rate, z, T, 40 + rate * 3 + z)
