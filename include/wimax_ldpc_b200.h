@@ -133,6 +133,13 @@ WLDPC_API int wldpc_decode_batch_device(wldpc_decoder* dec, const float* llr, in
  * status are nullable (frames entries each). */
 WLDPC_API int wldpc_decode_batch_host(wldpc_decoder* dec, float* rx_codewords, int8_t* decoded, uint32_t* num_errors,
                             int32_t* status, size_t frames);
+/* As wldpc_decode_batch_host without the posterior: llr is read only and
+ * only the hard decisions (and num_errors / status, nullable) come back, the
+ * outputs that BER_runner (reference lib/BER_runner.cc:194-199) and
+ * test_decoder (reference lib/decode_example.cc:128-148) use. It moves n
+ * bytes per frame back to the host instead of 5n. Synchronous. */
+WLDPC_API int wldpc_decode_batch_host_hard(wldpc_decoder* dec, const float* llr, int8_t* decoded,
+                                           uint32_t* num_errors, int32_t* status, size_t frames);
 
 /* Batch form of decode(int8_t*, int8_t*) over host buffers (frames x n bytes
  * in and out; num_errors nullable), as the reference's test_decoder drives it
@@ -146,6 +153,16 @@ WLDPC_API int wldpc_syndrome_batch_host(wldpc_decoder* dec, const int8_t* bits, 
 /* Waits for the device and reports a device-side error (WLDPC_ERR_TIMEOUT)
  * recorded by earlier launches of this decoder. */
 WLDPC_API int wldpc_decoder_synchronize(wldpc_decoder* dec);
+
+/* No counterpart in the reference (it has no device waits): a test hook that
+ * sets how many times the decode kernel polls the barrier of its frame
+ * staging copy before giving up (default WLDPC_WAIT_LIMIT_DEFAULT, well under
+ * a second). With 0 every launch gives up at once: it records a timeout,
+ * waits (with the default bound) for its copy to land and exits, and the
+ * next synchronising call returns WLDPC_ERR_TIMEOUT with the context intact.
+ * Outputs of such a launch are undefined. */
+#define WLDPC_WAIT_LIMIT_DEFAULT (1u << 22)
+WLDPC_API int wldpc_decoder_set_wait_limit(wldpc_decoder* dec, unsigned polls);
 
 /* ---------------------------------------------------------------- encoder */
 
@@ -227,6 +244,10 @@ WLDPC_API int wldpc_lms_decode_device(wldpc_lms* h, const float* llr, int8_t* de
 /* Decode host buffers (posterior written back; num_errors = syndrome failed). */
 WLDPC_API int wldpc_lms_decode_host(wldpc_lms* h, float* rx_codewords, int8_t* decoded, uint32_t* num_errors,
                                     int32_t* status, size_t frames);
+/* The same without the posterior (llr read only; hard decisions, num_errors
+ * and status back), as wldpc_decode_batch_host_hard. */
+WLDPC_API int wldpc_lms_decode_host_hard(wldpc_lms* h, const float* llr, int8_t* decoded, uint32_t* num_errors,
+                                         int32_t* status, size_t frames);
 /* Training loss (mean BCE over iterations, bits and frames; positive LLR =
  * bit 1) and its gradient table for host frames (llr, transmitted codeword
  * bits 0/1). Synchronous. */
@@ -270,10 +291,13 @@ WLDPC_API int wldpc_lms_apply_grad(wldpc_lms* h, const float* grad, float lr, vo
  * floats) receives the posterior, decoded the hard bits, num_errors (nullable)
  * the per-frame reference return values. The staging must fit the scratch
  * (about 5n bytes per frame: at most 90 frames at z=96, 363 at z=24); larger requests
- * return WLDPC_ERR_SCRATCH. The first call on a device looks up the scratch
- * address and should come before any stream capture. All calls share the
- * scratch: calls that overlap on the GPU race and must be serialised. Runs on
- * the default stream and returns when the results are in host memory. */
+ * return WLDPC_ERR_SCRATCH. Every call looks up the scratch's device address
+ * (which allocates nothing), so a device reset between calls is harmless; the
+ * first call on a device also loads the module there and should come before
+ * any stream capture. All calls share the scratch: calls that overlap on the
+ * GPU race and must be serialised. Runs on the default stream and returns
+ * when the results are in host memory; on a CUDA error it first waits for the
+ * copies it queued. */
 WLDPC_API int wldpc_decode_host_noalloc(int rate, unsigned z, unsigned max_iter, float* rx_codewords,
                                         int8_t* decoded, uint32_t* num_errors, size_t frames);
 

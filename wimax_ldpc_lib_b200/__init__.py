@@ -25,7 +25,8 @@ MODE_NMS, MODE_OMS, MODE_MS = 0, 1, 2
 LMS_F32, LMS_F16X2 = 0, 1   # learned-decoder inference arithmetic (wldpc_lms_set_precision)
 
 OK = 0
-ERR_ARG, ERR_CODE, ERR_CUDA, ERR_NO_DEVICE, ERR_TIMEOUT, ERR_UNSUPPORTED = -1, -2, -3, -4, -5, -6
+ERR_ARG, ERR_CODE, ERR_CUDA, ERR_NO_DEVICE, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_SCRATCH = -1, -2, -3, -4, -5, -6, -7
+WAIT_LIMIT_DEFAULT = 1 << 22   # WLDPC_WAIT_LIMIT_DEFAULT
 
 _p = ctypes.c_void_p
 _i = ctypes.c_int
@@ -73,6 +74,8 @@ def _lib():
     L.wldpc_decoder_compute_syndrome.argtypes = [_p, _p, _i, ctypes.POINTER(_u)]
     L.wldpc_decode_batch_device.argtypes = [_p, _p, _p, _p, _p, _sz, _p]
     L.wldpc_decode_batch_host.argtypes = [_p, _p, _p, _p, _p, _sz]
+    L.wldpc_decode_batch_host_hard.argtypes = [_p, _p, _p, _p, _p, _sz]
+    L.wldpc_decoder_set_wait_limit.argtypes = [_p, _u]
     L.wldpc_decoder_synchronize.argtypes = [_p]
     L.wldpc_encoder_create.argtypes = [_i, _u, _u, ctypes.POINTER(_p)]
     L.wldpc_encoder_destroy.argtypes = [_p]
@@ -88,6 +91,7 @@ def _lib():
     L.wldpc_lms_set_cap.argtypes = [_p, _u]
     L.wldpc_lms_set_precision.argtypes = [_p, _i]
     L.wldpc_lms_decode_host.argtypes = [_p, _p, _p, _p, _p, _sz]
+    L.wldpc_lms_decode_host_hard.argtypes = [_p, _p, _p, _p, _p, _sz]
     L.wldpc_lms_loss_grad.argtypes = [_p, _p, _p, _sz, _p, ctypes.POINTER(ctypes.c_double)]
     L.wldpc_lms_train.argtypes = [_p, _u, _u, ctypes.c_float, ctypes.c_float, ctypes.c_uint64, ctypes.c_uint64,
                                   ctypes.c_float, _p]
@@ -226,11 +230,21 @@ class Decoder:
         _check(_lib().wldpc_decode_batch_host(self._h, ptr(rx), ptr(decoded), ptr(num_errors), ptr(status),
                                               frames), "decode_batch_host")
 
+    def decode_host_hard_into(self, llr, decoded, num_errors=None, status=None):
+        """Host batch without the posterior (llr is read only; numpy or pinned torch CPU tensors)."""
+        ptr = _np_ptr if isinstance(llr, np.ndarray) else _t_ptr
+        _check(_lib().wldpc_decode_batch_host_hard(self._h, ptr(llr), ptr(decoded), ptr(num_errors), ptr(status),
+                                                   llr.shape[0]), "decode_batch_host_hard")
+
     def decode_device(self, llr, decoded, posterior=None, status=None, stream=None):
         """torch CUDA tensors, asynchronous on `stream` (default: torch's current stream)."""
         frames = llr.shape[0]
         _check(_lib().wldpc_decode_batch_device(self._h, _t_ptr(llr), _t_ptr(decoded), _t_ptr(posterior),
                                                 _t_ptr(status), frames, _stream_ptr(stream)), "decode_batch_device")
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Test hook: polls of the kernel's staging wait (0 = time out at once)."""
+        _check(_lib().wldpc_decoder_set_wait_limit(self._h, polls), "set_wait_limit")
 
     def synchronize(self):
         _check(_lib().wldpc_decoder_synchronize(self._h), "synchronize")
@@ -406,6 +420,18 @@ class LearnedDecoder:
         _check(_lib().wldpc_lms_decode_host(self._h, _np_ptr(post), _np_ptr(dec), _np_ptr(ne), _np_ptr(st), frames),
                "lms decode_host")
         return post, dec, ne, st
+
+    def decode_host_into(self, rx, decoded, num_errors=None, status=None):
+        """In-place host batch (posterior written back into rx); numpy or pinned torch CPU tensors."""
+        ptr = _np_ptr if isinstance(rx, np.ndarray) else _t_ptr
+        _check(_lib().wldpc_lms_decode_host(self._h, ptr(rx), ptr(decoded), ptr(num_errors), ptr(status),
+                                            rx.shape[0]), "lms decode_host")
+
+    def decode_host_hard_into(self, llr, decoded, num_errors=None, status=None):
+        """Host batch without the posterior (llr is read only)."""
+        ptr = _np_ptr if isinstance(llr, np.ndarray) else _t_ptr
+        _check(_lib().wldpc_lms_decode_host_hard(self._h, ptr(llr), ptr(decoded), ptr(num_errors), ptr(status),
+                                                 llr.shape[0]), "lms decode_host_hard")
 
     def loss_grad(self, llr: np.ndarray, codeword: np.ndarray):
         l = np.ascontiguousarray(llr, np.float32)

@@ -69,9 +69,23 @@ struct DevBuf {
 
 }  // namespace
 
+/* An error after copies were queued on the host-batch pipeline streams: wait
+ * for them (their results are not used) so that none writes into the caller's
+ * buffers after the call has returned. */
+template <int S>
+static int drain_pipe(cudaStream_t (&pipe)[S], int rc)
+{
+    cudaGetLastError();
+    for (cudaStream_t p : pipe)
+        if (p) cudaStreamSynchronize(p);
+    cudaGetLastError();
+    return rc;
+}
+
 struct wldpc_decoder {
     int rate, z, mode;
     unsigned max_iter;
+    unsigned wait_limit = kWaitLimit;   /* polls of the kernel's staging wait (test hook) */
     CodeDesc code;
     cudaStream_t stream = nullptr;
     cudaStream_t pipe[kHostStages] = {};
@@ -116,7 +130,7 @@ const char* wldpc_strerror(int code)
     }
 }
 
-int wldpc_version(void) { return 10100; }   /* 1.1.0: wldpc_lms_set_precision */
+int wldpc_version(void) { return 10200; }   /* 1.2.0: hard-decision host decodes, wait-limit hook */
 
 int wldpc_code_info_get(int rate, unsigned z, wldpc_code_info* out)
 {
@@ -214,6 +228,7 @@ static int decode_launch(wldpc_decoder* d, const float* llr, int8_t* hard, float
     a.err = d->err;
     a.frames = (long long)frames;
     a.max_iter = (int)d->max_iter;
+    a.wait_limit = d->wait_limit;
     return launch_tdmp(d->rate, d->z, d->mode, a, st) == cudaSuccess ? WLDPC_OK : WLDPC_ERR_CUDA;
 }
 
@@ -236,6 +251,15 @@ int wldpc_decode_batch_device(wldpc_decoder* d, const float* llr, int8_t* decode
         return WLDPC_ERR_ARG;
     if (frames == 0) return WLDPC_OK;
     return decode_launch(d, llr, decoded, posterior, status, frames, (cudaStream_t)stream);
+}
+
+static_assert(kWaitLimit == WLDPC_WAIT_LIMIT_DEFAULT, "the header's default wait limit is the kernels'");
+
+int wldpc_decoder_set_wait_limit(wldpc_decoder* d, unsigned polls)
+{
+    if (!d) return WLDPC_ERR_ARG;
+    d->wait_limit = polls;
+    return WLDPC_OK;
 }
 
 int wldpc_decoder_synchronize(wldpc_decoder* d)
@@ -363,9 +387,9 @@ int wldpc_syndrome_batch_host(wldpc_decoder* d, const int8_t* bits, int exit_ear
 
 /* Host batch: chunks of kHostChunk frames rotate over kHostStages streams so
  * that the copy-in of one chunk, the kernel of another and the copy-out of a
- * third overlap. */
-int wldpc_decode_batch_host(wldpc_decoder* d, float* rx, int8_t* decoded, uint32_t* num_errors,
-                            int32_t* status, size_t frames)
+ * third overlap. post (nullable) receives the posterior; it may alias rx. */
+static int decode_host_pipeline(wldpc_decoder* d, const float* rx, float* post, int8_t* decoded,
+                                uint32_t* num_errors, int32_t* status, size_t frames)
 {
     if (!d || (frames && (!rx || !decoded))) return WLDPC_ERR_ARG;
     if (frames == 0) return WLDPC_OK;
@@ -389,19 +413,36 @@ int wldpc_decode_batch_host(wldpc_decoder* d, float* rx, int8_t* decoded, uint32
         const int s = (int)(idx % kHostStages);
         const size_t nf = frames - f0 < chunk ? frames - f0 : chunk;
         cudaStream_t st = d->pipe[s];
-        CU(cudaMemcpyAsync(d->pllr[s].p, rx + f0 * n, nf * n * 4, cudaMemcpyHostToDevice, st));
-        if ((rc = decode_launch(d, (const float*)d->pllr[s].p, (int8_t*)d->phard[s].p, (float*)d->pllr[s].p,
-                                (int32_t*)d->pstatus[s].p, nf, st)))
-            return rc;
-        CU(cudaMemcpyAsync(rx + f0 * n, d->pllr[s].p, nf * n * 4, cudaMemcpyDeviceToHost, st));
-        CU(cudaMemcpyAsync(decoded + f0 * n, d->phard[s].p, nf * n, cudaMemcpyDeviceToHost, st));
-        if (st_host) CU(cudaMemcpyAsync(st_host + f0, d->pstatus[s].p, nf * 4, cudaMemcpyDeviceToHost, st));
+        if (cudaMemcpyAsync(d->pllr[s].p, rx + f0 * n, nf * n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            return drain_pipe(d->pipe, WLDPC_ERR_CUDA);
+        if ((rc = decode_launch(d, (const float*)d->pllr[s].p, (int8_t*)d->phard[s].p,
+                                post ? (float*)d->pllr[s].p : nullptr, (int32_t*)d->pstatus[s].p, nf, st)))
+            return drain_pipe(d->pipe, rc);
+        if ((post &&
+             cudaMemcpyAsync(post + f0 * n, d->pllr[s].p, nf * n * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) ||
+            cudaMemcpyAsync(decoded + f0 * n, d->phard[s].p, nf * n, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            (st_host &&
+             cudaMemcpyAsync(st_host + f0, d->pstatus[s].p, nf * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess))
+            return drain_pipe(d->pipe, WLDPC_ERR_CUDA);
     }
-    for (int s = 0; s < kHostStages; s++) CU(cudaStreamSynchronize(d->pipe[s]));
+    for (int s = 0; s < kHostStages; s++)
+        if (cudaStreamSynchronize(d->pipe[s]) != cudaSuccess) return drain_pipe(d->pipe, WLDPC_ERR_CUDA);
     if ((rc = read_err(d))) return rc;
     if (num_errors)
         for (size_t f = 0; f < frames; f++) num_errors[f] = ref_return(d, st_host[f]);
     return WLDPC_OK;
+}
+
+int wldpc_decode_batch_host(wldpc_decoder* d, float* rx, int8_t* decoded, uint32_t* num_errors,
+                            int32_t* status, size_t frames)
+{
+    return decode_host_pipeline(d, rx, rx, decoded, num_errors, status, frames);
+}
+
+int wldpc_decode_batch_host_hard(wldpc_decoder* d, const float* llr, int8_t* decoded, uint32_t* num_errors,
+                                 int32_t* status, size_t frames)
+{
+    return decode_host_pipeline(d, llr, nullptr, decoded, num_errors, status, frames);
 }
 
 /* ------------------------------------------------------------- encoder */

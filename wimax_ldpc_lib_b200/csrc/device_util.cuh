@@ -132,11 +132,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase)
 
 /* Bounded wait on an mbarrier phase. Each try_wait blocks for a hardware
  * time slice, so kWaitLimit tries bound the wait to well under a second on a
- * healthy GPU; on expiry the caller records kErrWaitTimeout and bails out. */
+ * healthy GPU; on expiry the caller records kErrWaitTimeout and bails out.
+ * limit = 0 gives up at once (the decoders' wait-limit test hook uses it). */
 constexpr uint32_t kWaitLimit = 1u << 22;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t limit = kWaitLimit)
 {
-    for (uint32_t i = 0; i < kWaitLimit; ++i)
+    for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, phase)) return true;
     return false;
 }

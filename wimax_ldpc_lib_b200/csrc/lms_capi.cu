@@ -335,9 +335,10 @@ int wldpc_lms_set_cap(wldpc_lms* h, unsigned cap)
 }
 
 /* Host batch: chunks rotate over kHostStages streams so that copies and
- * kernels of neighbouring chunks overlap (as wldpc_decode_batch_host). */
-int wldpc_lms_decode_host(wldpc_lms* h, float* rx, int8_t* decoded, uint32_t* num_errors, int32_t* status,
-                          size_t frames)
+ * kernels of neighbouring chunks overlap (as wldpc_decode_batch_host). post
+ * (nullable) receives the posterior; it may alias rx. */
+static int lms_decode_host_pipeline(wldpc_lms* h, const float* rx, float* post, int8_t* decoded,
+                                    uint32_t* num_errors, int32_t* status, size_t frames)
 {
     if (!h || (frames && (!rx || !decoded))) return WLDPC_ERR_ARG;
     if (frames == 0) return WLDPC_OK;
@@ -356,20 +357,33 @@ int wldpc_lms_decode_host(wldpc_lms* h, float* rx, int8_t* decoded, uint32_t* nu
         st_local.resize(frames);
         st = st_local.data();
     }
+    /* an error after copies were queued: wait for them (results unused) so
+     * that none writes into the caller's buffers after the call returns */
+    auto drain = [h](int code) {
+        cudaGetLastError();
+        for (cudaStream_t p : h->pipe)
+            if (p) cudaStreamSynchronize(p);
+        cudaGetLastError();
+        return code;
+    };
     size_t idx = 0;
     for (size_t f0 = 0; f0 < frames; f0 += chunk, idx++) {
         const int s = (int)(idx % kHostStages);
         const size_t nf = frames - f0 < chunk ? frames - f0 : chunk;
         cudaStream_t ps = h->pipe[s];
-        CU(cudaMemcpyAsync(h->pllr[s].p, rx + f0 * n, nf * n * 4, cudaMemcpyHostToDevice, ps));
-        if ((rc = lms_launch_decode(h, (const float*)h->pllr[s].p, (int8_t*)h->phard[s].p, (float*)h->pllr[s].p,
-                                    (int32_t*)h->pstat[s].p, nf, ps)))
-            return rc;
-        CU(cudaMemcpyAsync(rx + f0 * n, h->pllr[s].p, nf * n * 4, cudaMemcpyDeviceToHost, ps));
-        CU(cudaMemcpyAsync(decoded + f0 * n, h->phard[s].p, nf * n, cudaMemcpyDeviceToHost, ps));
-        if (st) CU(cudaMemcpyAsync(st + f0, h->pstat[s].p, nf * 4, cudaMemcpyDeviceToHost, ps));
+        if (cudaMemcpyAsync(h->pllr[s].p, rx + f0 * n, nf * n * 4, cudaMemcpyHostToDevice, ps) != cudaSuccess)
+            return drain(WLDPC_ERR_CUDA);
+        if ((rc = lms_launch_decode(h, (const float*)h->pllr[s].p, (int8_t*)h->phard[s].p,
+                                    post ? (float*)h->pllr[s].p : nullptr, (int32_t*)h->pstat[s].p, nf, ps)))
+            return drain(rc);
+        if ((post &&
+             cudaMemcpyAsync(post + f0 * n, h->pllr[s].p, nf * n * 4, cudaMemcpyDeviceToHost, ps) != cudaSuccess) ||
+            cudaMemcpyAsync(decoded + f0 * n, h->phard[s].p, nf * n, cudaMemcpyDeviceToHost, ps) != cudaSuccess ||
+            (st && cudaMemcpyAsync(st + f0, h->pstat[s].p, nf * 4, cudaMemcpyDeviceToHost, ps) != cudaSuccess))
+            return drain(WLDPC_ERR_CUDA);
     }
-    for (int s = 0; s < kHostStages; s++) CU(cudaStreamSynchronize(h->pipe[s]));
+    for (int s = 0; s < kHostStages; s++)
+        if (cudaStreamSynchronize(h->pipe[s]) != cudaSuccess) return drain(WLDPC_ERR_CUDA);
     unsigned e = 0;
     CU(cudaMemcpy(&e, h->err, 4, cudaMemcpyDeviceToHost));
     if (e) {
@@ -379,6 +393,18 @@ int wldpc_lms_decode_host(wldpc_lms* h, float* rx, int8_t* decoded, uint32_t* nu
     if (num_errors)
         for (size_t f = 0; f < frames; f++) num_errors[f] = (uint32_t)((st[f] >> 16) & 1);
     return WLDPC_OK;
+}
+
+int wldpc_lms_decode_host(wldpc_lms* h, float* rx, int8_t* decoded, uint32_t* num_errors, int32_t* status,
+                          size_t frames)
+{
+    return lms_decode_host_pipeline(h, rx, rx, decoded, num_errors, status, frames);
+}
+
+int wldpc_lms_decode_host_hard(wldpc_lms* h, const float* llr, int8_t* decoded, uint32_t* num_errors,
+                               int32_t* status, size_t frames)
+{
+    return lms_decode_host_pipeline(h, llr, nullptr, decoded, num_errors, status, frames);
 }
 
 /* one training forward/backward over `frames` frames already on the device;

@@ -13,18 +13,22 @@
  * posterior and hard-bit staging) lives in g_noalloc_scratch, a file-scope
  * static __device__ array of WLDPC_NOALLOC_SCRATCH_BYTES (1 MiB). Every GPU
  * that loads the library holds it until the process exits. In host code the
- * array's name is only a host-side stand-in, so the device address is taken
- * with cudaGetSymbolAddress once per device (with that device current) and
- * cached; the first call on a device does this set-up, so that first call
- * should come before any stream capture. Requests whose staging does not fit
- * return WLDPC_ERR_SCRATCH before touching the GPU.
+ * array's name is only a host-side stand-in, so every call takes the device
+ * address with cudaGetSymbolAddress (with the caller's device current; the
+ * lookup allocates nothing). Looking it up on every call rather than caching
+ * it keeps the address right after the caller resets the device or recreates
+ * its primary context, which can move the array. The first call on a device
+ * also loads the module there, so that first call should come before any
+ * stream capture. Requests whose staging does not fit return
+ * WLDPC_ERR_SCRATCH before touching the GPU. If a copy or the launch fails
+ * after work was queued, the call waits for the queued copies to finish
+ * before it returns, so nothing writes into the caller's buffers afterwards.
  *
  * Every call shares the one array and leaves the last call's contents in it;
  * the error word is cleared at the start of each call. Calls that overlap on
  * the GPU (for example from two host threads at once) race on the array and
  * must be serialised by the caller.
  */
-#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -37,9 +41,6 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[WLDPC_NOALLOC_S
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::atomic<void*> g_scratch_addr[kMaxDevices];
-
 size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 /* device address of g_noalloc_scratch on the current device */
@@ -50,17 +51,23 @@ int scratch_address(void** out)
         cudaGetLastError();
         return WLDPC_ERR_NO_DEVICE;
     }
-    if (dev < 0 || dev >= kMaxDevices) return WLDPC_ERR_UNSUPPORTED;
-    void* p = g_scratch_addr[dev].load(std::memory_order_acquire);
-    if (!p) {
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-            cudaGetLastError();
-            return WLDPC_ERR_CUDA;
-        }
-        g_scratch_addr[dev].store(p, std::memory_order_release);
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+        cudaGetLastError();
+        return WLDPC_ERR_CUDA;
     }
     *out = p;
     return WLDPC_OK;
+}
+
+/* error after work was queued on st: let the queued copies finish (their
+ * result is not needed) so that none lands in the caller's buffers later */
+int fail_after_enqueue(cudaStream_t st)
+{
+    cudaGetLastError();
+    cudaStreamSynchronize(st);
+    cudaGetLastError();
+    return WLDPC_ERR_CUDA;
 }
 
 }  // namespace
@@ -96,10 +103,8 @@ extern "C" WLDPC_API int wldpc_decode_host_noalloc(int rate, unsigned z, unsigne
     const cudaStream_t st = 0;
 
     if (cudaMemsetAsync(err, 0, sizeof(unsigned), st) != cudaSuccess ||
-        cudaMemcpyAsync(llr, rx_codewords, frames * n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess) {
-        cudaGetLastError();
-        return WLDPC_ERR_CUDA;
-    }
+        cudaMemcpyAsync(llr, rx_codewords, frames * n * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return fail_after_enqueue(st);
     DecodeArgs a;
     a.llr = llr;
     a.hard = hard;
@@ -108,20 +113,15 @@ extern "C" WLDPC_API int wldpc_decode_host_noalloc(int rate, unsigned z, unsigne
     a.err = err;
     a.frames = (long long)frames;
     a.max_iter = (int)max_iter;
-    if (launch_tdmp(rate, (int)z, kNms, a, st) != cudaSuccess) {
-        cudaGetLastError();
-        return WLDPC_ERR_CUDA;
-    }
+    if (launch_tdmp(rate, (int)z, kNms, a, st) != cudaSuccess) return fail_after_enqueue(st);
     unsigned errword = 0;
     if (cudaMemcpyAsync(rx_codewords, llr, frames * n * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(decoded, hard, frames * n, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         (num_errors &&
          cudaMemcpyAsync(num_errors, status, frames * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) ||
         cudaMemcpyAsync(&errword, err, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess) {
-        cudaGetLastError();
-        return WLDPC_ERR_CUDA;
-    }
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return fail_after_enqueue(st);
     if (errword) return WLDPC_ERR_TIMEOUT;
     /* status words -> the reference's return values, in place */
     if (num_errors)
