@@ -76,6 +76,9 @@ def _lib():
     L.wldpc_decode_batch_host.argtypes = [_p, _p, _p, _p, _p, _sz]
     L.wldpc_decode_batch_host_hard.argtypes = [_p, _p, _p, _p, _p, _sz]
     L.wldpc_decoder_set_wait_limit.argtypes = [_p, _u]
+    L.wldpc_decode_bits_batch_host.argtypes = [_p, _p, _p, _p, _sz]
+    L.wldpc_syndrome_batch_host.argtypes = [_p, _p, _i, _p, _sz]
+    L.wldpc_encode_batch_host.argtypes = [_p, _p, _p, _sz]
     L.wldpc_decoder_synchronize.argtypes = [_p]
     L.wldpc_encoder_create.argtypes = [_i, _u, _u, ctypes.POINTER(_p)]
     L.wldpc_encoder_destroy.argtypes = [_p]
@@ -229,6 +232,23 @@ class Decoder:
         frames = rx.shape[0]
         _check(_lib().wldpc_decode_batch_host(self._h, ptr(rx), ptr(decoded), ptr(num_errors), ptr(status),
                                               frames), "decode_batch_host")
+
+    def decode_bits_host(self, bits: np.ndarray):
+        """Batch decode(int8_t*, int8_t*) of frames x n host bytes: (decoded, num_errors)."""
+        b = np.ascontiguousarray(bits, np.int8)
+        dec = np.empty(b.shape, np.int8)
+        ne = np.empty(b.shape[0], np.uint32)
+        _check(_lib().wldpc_decode_bits_batch_host(self._h, _np_ptr(b), _np_ptr(dec), _np_ptr(ne), b.shape[0]),
+               "decode_bits_batch_host")
+        return dec, ne
+
+    def syndrome_host(self, bits: np.ndarray, exit_early: bool = False) -> np.ndarray:
+        """Batch compute_syndrome over frames x n host bytes."""
+        b = np.ascontiguousarray(bits, np.int8)
+        out = np.empty(b.shape[0], np.uint32)
+        _check(_lib().wldpc_syndrome_batch_host(self._h, _np_ptr(b), int(exit_early), _np_ptr(out), b.shape[0]),
+               "syndrome_batch_host")
+        return out
 
     def decode_host_hard_into(self, llr, decoded, num_errors=None, status=None):
         """Host batch without the posterior (llr is read only; numpy or pinned torch CPU tensors)."""
@@ -465,6 +485,43 @@ class LearnedDecoder:
     def apply_grad(self, grad, lr: float = 1e-3, stream=None):
         """One Adam step with the gradient in `grad` (float32 CUDA tensor)."""
         _check(_lib().wldpc_lms_apply_grad(self._h, _t_ptr(grad), lr, _stream_ptr(stream)), "lms apply_grad")
+
+
+WEIGHTS_DIR = os.path.join(HERE, "weights")
+
+
+def learned_weights(rate: int, z: int, evaluated_only: bool = True):
+    """Shipped learned min-sum weights for (rate, z): the table trained at
+    that z, else the one trained at the nearest z of the same rate (the
+    weights are per iteration, layer and base column, so a table applies to
+    every z of its rate). Returns (meta, weights float32 [2][T][12][24],
+    source z), or (None, None, None) when the rate has no trained table or,
+    with evaluated_only, when a transferred table was never evaluated at that
+    z (weights/lms_transfer.json). meta["evaluation"] holds the held-out
+    evaluation at (rate, z) when there is one."""
+    import json
+    trained = []
+    for name in os.listdir(WEIGHTS_DIR) if os.path.isdir(WEIGHTS_DIR) else []:
+        parts = name[:-5].split("_") if name.startswith("lms_r") and name.endswith(".json") else []
+        if len(parts) == 4 and parts[1] == f"r{rate}" and parts[2].startswith("z"):
+            trained.append((int(parts[2][1:]), name))
+    if not trained:
+        return None, None, None
+    src_z, name = min(trained, key=lambda t: (abs(t[0] - z), -t[0]))
+    with open(os.path.join(WEIGHTS_DIR, name)) as f:
+        meta = json.load(f)
+    if src_z != z:
+        ev = None
+        tpath = os.path.join(WEIGHTS_DIR, "lms_transfer.json")
+        if os.path.exists(tpath):
+            with open(tpath) as f:
+                for c in json.load(f)["codes"]:
+                    if c["rate"] == rate and c["z"] == z and c["source_z"] == src_z:
+                        ev = {"points": c["points"], "source": c["source"]}
+        if ev is None and evaluated_only:
+            return None, None, None
+        meta = dict(meta, z=z, source_z=src_z, evaluation=ev)
+    return meta, np.array(meta["weights"], np.float32), src_z
 
 
 class BERRunner:

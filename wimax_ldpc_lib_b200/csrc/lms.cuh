@@ -75,15 +75,24 @@ struct LmsArgs {
     float2 wab[kLmsMaxIter][kLmsMaxBlocks];   /* (a, b) per (iteration, block): one 8-byte load per edge */
 };
 
+/* Frames (or frame pairs) per CTA for the learned decoders: 32/gcd(z, 32)
+ * of them make the CTA a whole number of warps; while that would exceed 384
+ * threads (the register file must hold a few such CTAs at ~128 registers per
+ * thread) or 100 KB of posteriors, halve it (the last warp is then partial). */
+constexpr int lms_group(int z, int frame_bytes)
+{
+    int g = 32 / gcd_c(z, 32);
+    while (g > 1 && (g * z > 384 || g * frame_bytes > 100 * 1024)) g /= 2;
+    return g;
+}
+
 template <int R, int Z>
 struct LmsShape {
     static constexpr int MB = kMb[R];
     static constexpr int NBLK = num_blocks(R);
     static constexpr int N = kNB * Z;
     static constexpr int E = NBLK * Z;
-    /* frames per CTA: whole warps when that fits in ~100 KB, else one */
-    static constexpr int GW = 32 / gcd_c(Z, 32);
-    static constexpr int G = GW * N * 4 <= 100 * 1024 ? GW : 1;
+    static constexpr int G = lms_group(Z, N * 4);   /* frames per CTA */
     static constexpr int THREADS = G * Z;
     static constexpr int SMEM = G * N * 4;
 };

@@ -79,14 +79,16 @@ struct Lms16Shape {
     static constexpr int MB = kMb[R];
     static constexpr int NBLK = num_blocks(R);
     static constexpr int N = kNB * Z;
-    static constexpr int GP = 32 / gcd_c(Z, 32);   /* frame pairs per CTA */
+    static constexpr int GP = lms_group(Z, N * 4);  /* frame pairs per CTA */
     static constexpr int THREADS = GP * Z;
     static constexpr int FRAMES = 2 * GP;
     static constexpr int SMEM = GP * N * 4;        /* static shared memory (posteriors) */
     /* resident CTAs per SM the register allocation must allow without spills:
-     * rate 1/2 (degree <= 7) 5, the higher rates (degree 10-20) 4, one fewer
-     * at z = 24 (four pairs per CTA need more index registers) */
-    static constexpr int MIN_CTAS = (R == 0 ? 5 : 4) - (Z == 24 ? 1 : 0);
+     * for 96-thread CTAs, rate 1/2 (degree <= 7) 5 and the higher rates
+     * (degree 10-20) 4, scaled down for larger CTAs, and one fewer when a CTA
+     * holds four or more pairs (they need more index registers) */
+    static constexpr int MIN_CTAS_RAW = (R == 0 ? 480 : 384) / THREADS - (GP >= 4 ? 1 : 0);
+    static constexpr int MIN_CTAS = MIN_CTAS_RAW < 1 ? 1 : MIN_CTAS_RAW;
 };
 
 /* packed binary16 arithmetic on 32-bit words (lane 0 = low half) */
@@ -264,10 +266,13 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
         });
         return acc & kH2Sign;
     };
-    /* CTA-wide failing-frame mask: bit 2g + lane */
+    /* CTA-wide failing-frame mask: bit 2g + lane. When TH is not a multiple
+     * of 32 the last warp is partial and its reduction covers only its lanes. */
+    constexpr unsigned kTailLanes = TH % 32;
+    const unsigned wmask = (kTailLanes == 0 || tid < TH - (int)kTailLanes) ? 0xffffffffu : (1u << kTailLanes) - 1u;
     auto frame_fail = [&](uint32_t acc, int slot) -> unsigned {
         unsigned bits = (((acc >> 15) & 1u) | ((acc >> 30) & 2u)) << (2 * g);
-        bits = __reduce_or_sync(0xffffffffu, bits);
+        bits = __reduce_or_sync(wmask, bits);
         if ((tid & 31) == 0 && bits) atomicOr(&s_fail[slot], bits);
         __syncthreads();
         return s_fail[slot];

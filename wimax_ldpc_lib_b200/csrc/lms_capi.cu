@@ -22,12 +22,17 @@ using namespace wldpc;
 extern "C" int wldpc_internal_nullspace_frames(int rate, int z, const wldpc::FramegenArgs& a, cudaStream_t st);
 
 namespace wldpc {
-extern const LmsLaunch kLms_r0[kLmsNumZ];
-extern const LmsLaunch kLms_r1[kLmsNumZ];
-extern const LmsLaunch kLms_r2[kLmsNumZ];
-extern const LmsLaunch kLms_r3[kLmsNumZ];
-extern const LmsLaunch kLms_r4[kLmsNumZ];
-extern const LmsLaunch kLms_r5[kLmsNumZ];
+/* dispatch rows defined by the 12 compilations of lms_instances.cuh */
+#define WLDPC_LMS_HALVES(R)                             \
+    extern const LmsLaunch kLms_r##R##_h0[kLmsHalf0]; \
+    extern const LmsLaunch kLms_r##R##_h1[kNumZ - kLmsHalf0];
+WLDPC_LMS_HALVES(0)
+WLDPC_LMS_HALVES(1)
+WLDPC_LMS_HALVES(2)
+WLDPC_LMS_HALVES(3)
+WLDPC_LMS_HALVES(4)
+WLDPC_LMS_HALVES(5)
+#undef WLDPC_LMS_HALVES
 
 /* Column sums of the per-frame gradients in frame order (deterministic),
  * the batch loss, then Adam; one thread per weight. */
@@ -55,11 +60,13 @@ __global__ void lms_reduce_adam_kernel(const __grid_constant__ AdamArgs a)
 
 const LmsLaunch* lms_entry(int rate, int z)
 {
-    static const LmsLaunch* const t[kRates] = {kLms_r0, kLms_r1, kLms_r2, kLms_r3, kLms_r4, kLms_r5};
-    if (!valid_rate(rate)) return nullptr;
-    for (int i = 0; i < kLmsNumZ; i++)
-        if (t[rate][i].z == z) return &t[rate][i];
-    return nullptr;
+    static const LmsLaunch* const t[kRates][2] = {{kLms_r0_h0, kLms_r0_h1}, {kLms_r1_h0, kLms_r1_h1},
+                                                  {kLms_r2_h0, kLms_r2_h1}, {kLms_r3_h0, kLms_r3_h1},
+                                                  {kLms_r4_h0, kLms_r4_h1}, {kLms_r5_h0, kLms_r5_h1}};
+    if (!valid_rate(rate) || !valid_z(z)) return nullptr;
+    const int zi = z_index(z);
+    const LmsLaunch* e = zi < kLmsHalf0 ? &t[rate][0][zi] : &t[rate][1][zi - kLmsHalf0];
+    return e->z == z ? e : nullptr;
 }
 }  // namespace wldpc
 

@@ -7,7 +7,9 @@
 
 namespace wldpc {
 
-constexpr int kLmsNumZ = 3;   /* z = 24, 48, 96 */
+/* every code has learned kernels: 19 expansion factors, instantiated in two
+ * halves per rate (lms_instances.cuh), z = 24..56 and z = 60..96 */
+constexpr int kLmsHalf0 = 9;
 
 struct LmsLaunch {
     int z;

@@ -2,6 +2,7 @@
 records where they ship.
 
   python -m wimax_ldpc_lib_b200.eval_lms weights/lms_r0_z96_T8.json [--frames 1048576]
+  python -m wimax_ldpc_lib_b200.eval_lms --transfer [--frames 262144]
 
 For every Eb/N0 point (default 1.0 to 3.0 dB in 0.25 dB steps) it generates
 held-out frames on the device (a seed and frame counters disjoint from
@@ -15,6 +16,13 @@ weights ship at a point and cap when their frame errors on those frames are
 no more than the plain decoder's at the same cap and they need fewer
 iterations on average (plain min-sum stays the yardstick and the fallback). The
 table is written back into the weight file under "evaluation".
+
+--transfer evaluates every code without weights of its own (the 19 z values
+of each rate other than the trained z = 48 and z = 96) with the weights
+trained at the nearest z of the same rate -- the weights are per (iteration,
+layer, base column), so they apply to any z -- by the same rule, and writes
+weights/lms_transfer.json (which learned_weights() reads to say where a
+transferred table ships).
 """
 from __future__ import annotations
 
@@ -106,14 +114,54 @@ def evaluate(meta, frames=1 << 20, batch=1 << 18, points=None, log=print):
     return rows
 
 
+def transfer(frames, out, log=print):
+    """Every (rate, z) without trained weights, with the nearest trained z's table."""
+    import time
+    import torch
+    res = {"format": "wimax_ldpc_lib_b200 learned-weight transfer evaluation v1", "seed": EVAL_SEED,
+           "frames_per_point": frames, "device": torch.cuda.get_device_name(0),
+           "rule": "weights trained at the nearest z of the same rate; ship at a point and cap where learned frame "
+                   "errors <= plain frame errors at that cap on the same held-out frames and learned mean "
+                   "iterations < plain mean iterations", "codes": []}
+    t0 = time.time()
+    for rate in range(6):
+        for z in wl.Z_VALUES:
+            meta, _, src_z = wl.learned_weights(rate, z, evaluated_only=False)
+            if meta is None or src_z == z:
+                continue
+            m = dict(meta, z=z)
+            rows = evaluate(m, frames, batch=frames, log=lambda *a: None)
+            ship10 = sum(r["ship_cap10"] for r in rows)
+            ship16 = sum(r.get("ship_cap10_f16x2", False) for r in rows)
+            res["codes"].append({"rate": rate, "z": z, "source_z": src_z,
+                                 "source": f"lms_r{rate}_z{src_z}_T{meta['iterations']}.json",
+                                 "ships_cap10": ship10, "ships_cap10_f16x2": ship16, "points": rows})
+            P = rows[len(rows) // 2]
+            log(f"rate {wl.RATE_NAMES[rate]:5s} z={z:2d} from z={src_z}: ships at {ship10}/{len(rows)} points "
+                f"(binary16 {ship16}); mid point {P['ebno_db']:.2f} dB learned10 FER {P['learned10']['fer']:.2e} "
+                f"it {P['learned10']['mean_iterations']:.2f} vs plain10 {P['plain10']['fer']:.2e} "
+                f"it {P['plain10']['mean_iterations']:.2f}")
+            res["seconds"] = round(time.time() - t0, 1)
+            with open(out, "w") as f:
+                json.dump(res, f)
+    print(f"wrote {out}")
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("weights")
-    ap.add_argument("--frames", type=int, default=1 << 20)
+    ap.add_argument("weights", nargs="?")
+    ap.add_argument("--frames", type=int, default=None)
     ap.add_argument("--points", type=float, nargs="*", default=None)
+    ap.add_argument("--transfer", action="store_true", help="evaluate the codes without weights of their own")
     ap.add_argument("--out", default=None, help="where to write the weight file with its evaluation "
                                                 "(default: in place)")
     args = ap.parse_args()
+    if args.transfer:
+        transfer(args.frames or (1 << 18), args.out or os.path.join(HERE, "weights", "lms_transfer.json"))
+        return
+    if not args.weights:
+        ap.error("a weight file, or --transfer")
+    args.frames = args.frames or (1 << 20)
     with open(args.weights) as f:
         meta = json.load(f)
     rows = evaluate(meta, args.frames, points=args.points)
