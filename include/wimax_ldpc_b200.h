@@ -213,8 +213,9 @@ WLDPC_API int wldpc_framegen_device(int rate, unsigned z, uint64_t seed, uint64_
  * trained on the GPU by the library's own forward/backward kernels and Adam.
  * Weight tables are float[2][T][12][24]: a then b, [iteration][layer][column];
  * entries of all-zero blocks are ignored (returned as 0). Supported codes:
- * every rate at z = 24, 48, 96 (WLDPC_ERR_UNSUPPORTED otherwise); 3/4B
- * trains on null-space codewords. A new handle starts at a = 0.815, b = 0. */
+ * all 114 (every rate, z = 24..96 step 4); a table trained at one z applies
+ * to every z of its rate, since it is indexed by base column. 3/4B trains on
+ * null-space codewords. A new handle starts at a = 0.815, b = 0. */
 typedef struct wldpc_lms wldpc_lms;
 WLDPC_API int wldpc_lms_create(int rate, unsigned z, unsigned iterations, wldpc_lms** out);
 WLDPC_API int wldpc_lms_destroy(wldpc_lms* h);
