@@ -337,19 +337,29 @@ typedef struct wldpc_mixed wldpc_mixed;
 WLDPC_API int wldpc_mixed_create(unsigned max_iter, wldpc_mixed** out);
 WLDPC_API int wldpc_mixed_destroy(wldpc_mixed* h);
 /* variant[f]: code of frame f; offset[f]: element offset of frame f's n values
- * in llr / decoded / posterior (frames may be in any order). Asynchronous on
- * stream (ordered with it through events). */
+ * in llr / decoded / posterior (frames may be in any order), a multiple of 4
+ * so that every frame starts 16-byte aligned (frames of n = 24z values packed
+ * back to back satisfy it); llr and posterior 16-byte aligned, decoded 4.
+ * Asynchronous on stream (ordered with it through events). */
 WLDPC_API int wldpc_mixed_decode_device(wldpc_mixed* h, const uint8_t* variant, const int64_t* offset,
                                         const float* llr, int8_t* decoded, float* posterior, int32_t* status,
                                         size_t frames, void* stream);
-/* Waits for the handle's work; WLDPC_ERR_ARG if a frame had an invalid code. */
+/* Waits for the handle's work; WLDPC_ERR_ARG if a frame had an invalid code
+ * or an offset that is not a multiple of 4 (such frames are not decoded). */
 WLDPC_API int wldpc_mixed_synchronize(wldpc_mixed* h);
 /* The autotuner's knobs: CTA size (96 or 192 threads, which sets the frame
- * slots per CTA to threads / z) and frames per work item. */
+ * slots per CTA to threads / z), where each thread's compressed messages
+ * live (registers, or shared memory: fewer registers and more resident CTAs)
+ * and frames per work item (1..64). set_config / get_config leave the layout
+ * as it is. */
+#define WLDPC_MIXED_MSG_REGISTERS 0
+#define WLDPC_MIXED_MSG_SHARED 1
+WLDPC_API int wldpc_mixed_set_tuning(wldpc_mixed* h, int threads, int layout, int chunk);
+WLDPC_API int wldpc_mixed_get_tuning(wldpc_mixed* h, int* threads, int* layout, int* chunk);
 WLDPC_API int wldpc_mixed_set_config(wldpc_mixed* h, int threads, int chunk);
 WLDPC_API int wldpc_mixed_get_config(wldpc_mixed* h, int* threads, int* chunk);
-/* Times every (threads, chunk) candidate on the given batch (repeats launches
- * each) and keeps the fastest; *best_ms (nullable) gets its time. */
+/* Times every (threads, layout, chunk) candidate on the given batch (repeats
+ * launches each) and keeps the fastest; *best_ms (nullable) gets its time. */
 WLDPC_API int wldpc_mixed_autotune(wldpc_mixed* h, const uint8_t* variant, const int64_t* offset, const float* llr,
                                    int8_t* decoded, size_t frames, int repeats, float* best_ms);
 

@@ -41,8 +41,11 @@ def test_mixed_matches_specialised_decoders(wl, cuda, batch):
     ref_status = torch.empty(frames, dtype=torch.int32, device="cuda")
     decode_by_code(groups, llr, ref_hard, ref_status)
     mixed = wl.MixedDecoder(10)
-    for threads, chunk in [(96, 32), (192, 8), (96, 64)]:
-        mixed.set_config(threads, chunk)
+    R, S = wl.MIXED_MSG_REGISTERS, wl.MIXED_MSG_SHARED
+    # every CTA size and message layout; chunks from one frame per item to the maximum
+    for threads, layout, chunk in [(96, R, 32), (96, S, 8), (192, R, 64), (192, S, 16), (96, R, 1), (192, S, 3)]:
+        mixed.set_tuning(threads, layout, chunk)
+        assert mixed.tuning() == (threads, layout, chunk)
         for _ in range(2):   # capture, then replay
             hard = torch.zeros(llr.numel(), dtype=torch.int8, device="cuda")
             status = torch.full((frames,), -1, dtype=torch.int32, device="cuda")
@@ -50,8 +53,8 @@ def test_mixed_matches_specialised_decoders(wl, cuda, batch):
             mixed.decode_device(variants, offsets, llr, hard, post, status)
             torch.cuda.synchronize()
             mixed.synchronize()
-            assert torch.equal(hard, ref_hard), (threads, chunk)
-            assert torch.equal(status, ref_status), (threads, chunk)
+            assert torch.equal(hard, ref_hard), (threads, layout, chunk)
+            assert torch.equal(status, ref_status), (threads, layout, chunk)
 
 
 def test_mixed_matches_oracle_sample(wl, cuda, oracle, batch):
@@ -80,10 +83,23 @@ def test_mixed_autotune_and_bad_code(wl, cuda, batch):
     mixed = wl.MixedDecoder(10)
     hard = torch.empty(llr.numel(), dtype=torch.int8, device="cuda")
     ms = mixed.autotune(variants, offsets, llr, hard, repeats=1)
-    assert ms > 0 and mixed.config()[0] in (96, 192)
+    threads, layout, chunk = mixed.tuning()
+    assert ms > 0 and threads in (96, 192) and layout in (0, 1) and chunk in (8, 16, 32, 64)
     bad = variants.clone()
     bad[0] = 200
     mixed.decode_device(bad, offsets, llr, hard)
     torch.cuda.synchronize()
     with pytest.raises(wl.LdpcError):
         mixed.synchronize()
+    # a frame that does not start on a 16-byte boundary is refused (and not decoded)
+    odd = offsets.clone()
+    odd[1] += 1
+    mixed.decode_device(variants, odd, llr, hard)
+    torch.cuda.synchronize()
+    with pytest.raises(wl.LdpcError) as e:
+        mixed.synchronize()
+    assert e.value.code == wl.ERR_ARG
+    mixed.decode_device(variants, offsets, llr, hard)   # and the handle still works
+    mixed.synchronize()
+    with pytest.raises(wl.LdpcError):
+        mixed.set_tuning(96, 0, 65)                        # at most 64 frames per work item

@@ -1,6 +1,7 @@
 /*
- * Mixed-code persistent decoder (see mixed.cuh): kernels, binning, CUDA-graph
- * capture, autotuning, and the C ABI (wldpc_mixed_*).
+ * Mixed-code persistent decoder (see mixed.cuh): binning kernels, CUDA-graph
+ * capture, autotuning, and the C ABI (wldpc_mixed_*). The decode kernels are
+ * in mixed_kernel.cuh, instantiated per rate by mixed_instances.cuh.
  */
 #include <chrono>
 #include <cstdint>
@@ -12,215 +13,20 @@
 
 #include "wimax_ldpc_b200.h"
 #include "codec_kernels.cuh"
-#include "mixed.cuh"
+#include "mixed_kernel.cuh"
 
 namespace wldpc {
 
-__constant__ MixedCode c_codes[kVariants];
-
-struct MixedSlots {
-    int frame[32];
-    int next;
-    unsigned fresh, fail;
-    int item;
-};
-
-/* Each thread's edge addresses for the current code, [block][thread] in
- * shared memory, computed once per work item: one 16-bit load per edge. */
-template <int R, int I, int E, int THREADS>
-__device__ __forceinline__ int mixed_var(const unsigned short* A)
-{
-    constexpr int b = block_index(R, I, E);
-    return A[b * THREADS + threadIdx.x];
-}
-
-template <int R, int THREADS>
-__device__ __forceinline__ void mixed_run_item(const MixedArgs& a, const MixedItem item, float* sp,
-                                               unsigned short* A, MixedSlots& S)
-{
-    constexpr int MB = kMb[R];
-    constexpr int NBLK = num_blocks(R);
-    const MixedCode& code = c_codes[item.variant];
-    const int z = code.z, n = code.n;
-    const int G = THREADS / z;
-    const int tid = threadIdx.x;
-    const int g = tid / z;
-    const int r = tid - g * z;
-    const bool in_slot = g < G;
-    float* P = sp + (in_slot ? g : 0) * n;
-    for (int b = 0; b < NBLK; b++) {
-        int t = r + (int)code.shift[b];
-        t = t >= z ? t - z : t;
-        A[b * THREADS + tid] = in_slot ? (unsigned short)(code.colz[b] + t) : (unsigned short)0;
-    }
-
-    float M1[MB], M2[MB];
-    uint32_t NEG[MB];
-    int frame = -1, iters = 0;
-    long long off = 0;
-    bool need_check = false;
-
-    if (tid == 0) {
-        S.next = 0;
-        for (int q = 0; q < G; q++) S.frame[q] = -1;
-    }
-    __syncthreads();
-    while (true) {
-        /* refill empty slots with the item's next frames */
-        if (tid == 0) {
-            unsigned fresh = 0;
-            for (int q = 0; q < G; q++)
-                if (S.frame[q] < 0 && S.next < item.count) {
-                    S.frame[q] = a.perm[item.start + S.next++];
-                    fresh |= 1u << q;
-                }
-            S.fresh = fresh;
-            S.fail = 0;
-        }
-        __syncthreads();
-        if (in_slot && ((S.fresh >> g) & 1u)) {
-            frame = S.frame[g];
-            off = a.offset[frame];
-            iters = 0;
-            need_check = true;
-            for (int c = 0; c < kNB; c++) P[c * z + r] = a.llr[off + c * z + r];
-#pragma unroll
-            for (int i = 0; i < MB; i++) { M1[i] = 0.0f; M2[i] = 0.0f; NEG[i] = 0u; }
-        }
-        __syncthreads();
-        /* syndrome of the slots loaded or iterated since their last check */
-        if (in_slot && frame >= 0 && need_check) {
-            unsigned fail = 0;
-            static_for<MB>([&](auto I) {
-                constexpr int d = layer_degree(R, I);
-                bool odd = (d & 1) != 0;   /* parity of the hard bits: d minus the negatives */
-                static_for<d>([&](auto E_) {
-                    odd = odd != (P[mixed_var<R, I, E_, THREADS>(A)] < 0.0f);
-                });
-                fail |= odd ? 1u : 0u;
-            });
-            if (fail) atomicOr(&S.fail, 1u << g);
-        }
-        __syncthreads();
-        if (in_slot && frame >= 0 && need_check) {
-            need_check = false;
-            const bool failed = (S.fail >> g) & 1u;
-            if (!failed || iters >= a.max_iter) {
-                for (int c = 0; c < kNB; c++) {
-                    const float p = P[c * z + r];
-                    a.hard[off + c * z + r] = p >= 0.0f ? 1 : 0;
-                    if (a.post) a.post[off + c * z + r] = p;
-                }
-                if (r == 0) {
-                    if (a.status) a.status[frame] = iters | ((failed ? 1 : 0) << 16);
-                    S.frame[g] = -1;
-                }
-                frame = -1;
-            }
-        }
-        __syncthreads();
-        bool any_empty = false, all_empty = true;
-        for (int q = 0; q < G; q++) {
-            any_empty |= S.frame[q] < 0;
-            all_empty &= S.frame[q] < 0;
-        }
-        const bool more = S.next < item.count;
-        __syncthreads();
-        if (all_empty && !more) break;
-        if (any_empty && more) continue;
-
-        /* one iteration of every occupied slot (all of them failed their check) */
-        const bool active = in_slot && frame >= 0;
-        static_for<MB>([&](auto I) {
-            constexpr int d = layer_degree(R, I);
-            if (active) {
-                float L[d];
-                uint32_t LC[d];
-                uint32_t sgn = 0;
-                float m1, m2;
-                const float oM1 = M1[I], oM2 = M2[I];
-                const uint32_t oNeg = NEG[I];
-                const int oIdx = (int)(oNeg >> 27);
-                /* the layer's edge addresses, loaded once for both passes */
-                int ad[d];
-                static_for<d>([&](auto E_) { ad[decltype(E_)::value] = mixed_var<R, I, decltype(E_)::value, THREADS>(A); });
-                static_for<d>([&](auto E_) {
-                    constexpr int e = decltype(E_)::value;
-                    const float x = P[ad[e]];
-                    const float mag = (oIdx == e) ? oM2 : oM1;
-                    const uint32_t sb = (oNeg << (32 - d + e)) & 0x80000000u;
-                    const float l = __fsub_rn(x, __uint_as_float(__float_as_uint(mag) | sb));
-                    L[e] = l;
-                    LC[e] = __float_as_uint(canon(l));
-                    sgn = __funnelshift_l(LC[e], sgn, 1);
-                });
-                /* the two smallest |L| from 10000.0f (reference lib/ldpc_decoder.cc:150,198) */
-                two_min_abs<0, d>(L, m1, m2);
-                m1 = fminf(m1, 10000.0f);
-                m2 = fminf(m2, 10000.0f);
-                const uint32_t flip = (uint32_t)((d & 1) ^ (__popc(sgn) & 1));
-                const uint32_t dmask = (d >= 32) ? 0xffffffffu : ((1u << d) - 1u);
-                const double D1 = __dmul_rn((double)m1, 0.815);
-                const double D2 = __dmul_rn((double)m2, 0.815);
-                const uint32_t fb = flip << 31;
-                const int h1 = __double2hiint(D1) ^ (int)fb, l1 = __double2loint(D1);
-                const int h2 = __double2hiint(D2) ^ (int)fb, l2 = __double2loint(D2);
-                int nIdx = 0;
-                static_for<d>([&](auto E_) {
-                    constexpr int e = decltype(E_)::value;
-                    const float l = L[e];
-                    const bool is_min = fabsf(l) == m1;
-                    nIdx = is_min ? e : nIdx;
-                    int hi = is_min ? h2 : h1;
-                    const int lo = is_min ? l2 : l1;
-                    hi ^= (int)(LC[e] & 0x80000000u);
-                    P[ad[e]] = __double2float_rn(__dadd_rn((double)l, __hiloint2double(hi, lo)));
-                });
-                M1[I] = __double2float_rn(D1);
-                M2[I] = __double2float_rn(D2);
-                NEG[I] = ((sgn ^ (flip ? dmask : 0u)) & dmask) | ((uint32_t)nIdx << 27);
-            }
-            __syncthreads();
-        });
-        if (active) {
-            iters++;
-            need_check = true;
-        }
-    }
-}
-
-/* One persistent kernel per rate: it takes work items of its rate from its
- * own queue until none are left. The register cap (80 per thread: 8 CTAs of
- * 96 or 4 of 192 threads per SM) trades a few spills in the 5/6 kernels for
- * more resident warps; the kernel is latency-bound, and this measured 18.6
- * against 16.2 info Gbit/s uncapped on the mixed batch. */
-template <int R, int THREADS>
-__global__ void __launch_bounds__(THREADS, (THREADS == 96 ? 8 : 4)) mixed_decode_kernel(const __grid_constant__ MixedArgs a)
-{
-    extern __shared__ __align__(16) float smem_mixed[];   /* posteriors, then the address table */
-    __shared__ MixedSlots S;
-    unsigned short* A = reinterpret_cast<unsigned short*>(smem_mixed + 24 * THREADS);
-    const MixedItem* items = a.items + (long long)R * a.items_per_rate;
-    while (true) {
-        if (threadIdx.x == 0) S.item = atomicAdd(&a.queue[R], 1);
-        __syncthreads();
-        const int k = S.item;
-        __syncthreads();
-        if (k >= a.num_items[R]) break;
-        mixed_run_item<R, THREADS>(a, items[k], smem_mixed, A, S);
-        __syncthreads();
-    }
-}
-
 /* ---- binning: counts, plan (prefix sums and work items), scatter ---- */
 
-__global__ void mixed_count_kernel(const uint8_t* __restrict__ variant, int* __restrict__ counts,
-                                   int* __restrict__ rank, long long frames, unsigned* err)
+__global__ void mixed_count_kernel(const uint8_t* __restrict__ variant, const long long* __restrict__ offset,
+                                   int* __restrict__ counts, int* __restrict__ rank, long long frames, unsigned* err)
 {
     for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < frames;
          f += (long long)gridDim.x * blockDim.x) {
         const int v = variant[f];
-        if (v >= kVariants) {
+        /* a frame must start 16-byte aligned (its bulk copy and vector stores) */
+        if (v >= kVariants || (offset[f] & 3) != 0 || offset[f] < 0) {
             atomicOr(err, kErrBadArgument);
             rank[f] = -1;
             continue;
@@ -295,49 +101,31 @@ struct MBuf {
     }
 };
 
-/* per device: the code table has been copied into c_codes */
-bool g_codes_uploaded[64] = {false};
-std::mutex g_codes_mutex;
-
-int upload_codes()
-{
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) {
-        cudaGetLastError();
-        return WLDPC_ERR_NO_DEVICE;
-    }
-    if (dev < 0 || dev >= 64) return WLDPC_ERR_UNSUPPORTED;
-    std::lock_guard<std::mutex> lock(g_codes_mutex);
-    if (g_codes_uploaded[dev]) return WLDPC_OK;
-    std::vector<MixedCode> t(kVariants);
-    for (int rate = 0; rate < kRates; rate++)
-        for (int zi = 0; zi < kNumZ; zi++) {
-            const int z = kZMin + kZStep * zi;
-            const CodeDesc c = make_code_desc(rate, z);
-            MixedCode& m = t[rate * kNumZ + zi];
-            memset(&m, 0, sizeof(m));
-            m.z = (unsigned short)z;
-            m.n = (unsigned short)c.n;
-            for (int b = 0; b < c.nblk; b++) {
-                m.colz[b] = (unsigned short)(c.col[b] * z);
-                m.shift[b] = c.shift[b];
-            }
-        }
-    if (cudaMemcpyToSymbol(c_codes, t.data(), sizeof(MixedCode) * kVariants) != cudaSuccess) {
-        cudaGetLastError();
-        return WLDPC_ERR_CUDA;
-    }
-    g_codes_uploaded[dev] = true;
-    return WLDPC_OK;
-}
+inline bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
 
 }  // namespace
 
+namespace wldpc {
+/* [threads 96 | 192][layout registers | shared], per rate (mixed_instances.cuh) */
+extern const MixedKernel kMixed_r0[2][2];
+extern const MixedKernel kMixed_r1[2][2];
+extern const MixedKernel kMixed_r2[2][2];
+extern const MixedKernel kMixed_r3[2][2];
+extern const MixedKernel kMixed_r4[2][2];
+extern const MixedKernel kMixed_r5[2][2];
+}  // namespace wldpc
+
+static MixedKernel mixed_kernel(int ti, int layout, int rate)
+{
+    static const MixedKernel (*const t[kRates])[2] = {kMixed_r0, kMixed_r1, kMixed_r2, kMixed_r3, kMixed_r4, kMixed_r5};
+    return t[rate][ti][layout];
+}
+
 struct wldpc_mixed {
     unsigned max_iter;
-    int threads = 96, chunk = 32;
+    int threads = 192, layout = kMsgShared, chunk = 16;
     int sms = 148;
-    int per_sm[2][kRates] = {};   /* resident CTAs per SM, [96 | 192 threads][rate] */
+    int per_sm[2][2][kRates] = {};   /* resident CTAs per SM, [96 | 192 threads][layout][rate] */
     cudaStream_t stream = nullptr;
     cudaStream_t rs[kRates] = {};
     cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_fork = nullptr, ev_join[kRates] = {};
@@ -349,20 +137,9 @@ struct wldpc_mixed {
     struct Key {
         const void *variant, *offset, *llr, *hard, *post, *status;
         size_t frames;
-        int threads, chunk;
+        int threads, layout, chunk;
         bool operator==(const Key& o) const { return memcmp(this, &o, sizeof(Key)) == 0; }
     } key{};
-};
-
-using MixedKernel = void (*)(const MixedArgs);
-/* dynamic shared memory of a CTA: posteriors (24 floats per thread) and the
- * 16-bit address table (96 blocks per thread) */
-static int mixed_smem(int threads) { return 24 * threads * 4 + 96 * threads * 2; }
-template <int T>
-struct MixedKernels {
-    static constexpr MixedKernel k[kRates] = {&mixed_decode_kernel<0, T>, &mixed_decode_kernel<1, T>,
-                                             &mixed_decode_kernel<2, T>, &mixed_decode_kernel<3, T>,
-                                             &mixed_decode_kernel<4, T>, &mixed_decode_kernel<5, T>};
 };
 
 static int mixed_enqueue(wldpc_mixed* h, const uint8_t* variant, const long long* offset, const float* llr,
@@ -373,7 +150,7 @@ static int mixed_enqueue(wldpc_mixed* h, const uint8_t* variant, const long long
     const long long per_rate = nf / chunk + kNumZ + 1;
     if (cudaMemsetAsync(h->counts.p, 0, sizeof(int) * kVariants, st) != cudaSuccess) return WLDPC_ERR_CUDA;
     const unsigned gb = (unsigned)((nf + 255) / 256 < 4096 ? (nf + 255) / 256 : 4096);
-    mixed_count_kernel<<<gb, 256, 0, st>>>(variant, (int*)h->counts.p, (int*)h->rank.p, nf, h->err);
+    mixed_count_kernel<<<gb, 256, 0, st>>>(variant, offset, (int*)h->counts.p, (int*)h->rank.p, nf, h->err);
     mixed_plan_kernel<<<1, 32, 0, st>>>((const int*)h->counts.p, (int*)h->base.p, (MixedItem*)h->items.p,
                                        (int*)h->nitems.p, (int*)h->queue.p, chunk, per_rate);
     mixed_scatter_kernel<<<gb, 256, 0, st>>>(variant, (const int*)h->rank.p, (const int*)h->base.p,
@@ -395,15 +172,15 @@ static int mixed_enqueue(wldpc_mixed* h, const uint8_t* variant, const long long
     a.max_iter = (int)h->max_iter;
     const int T = h->threads;
     const int ti = T == 96 ? 0 : 1;
-    const int smem = mixed_smem(T);
+    const int smem = mixed_smem_bytes(T, h->layout);
     /* fork: the six rate kernels run concurrently, then join back on st */
     if (cudaGetLastError() != cudaSuccess || cudaEventRecord(h->ev_fork, st) != cudaSuccess) return WLDPC_ERR_CUDA;
     /* every forked stream is joined back even when a step fails, so that a
      * capture in progress always ends with all its streams joined */
     int rc = WLDPC_OK;
     for (int rate = 0; rate < kRates; rate++) {
-        const MixedKernel k = ti == 0 ? MixedKernels<96>::k[rate] : MixedKernels<192>::k[rate];
-        const int per_sm = h->per_sm[ti][rate];
+        const MixedKernel k = mixed_kernel(ti, h->layout, rate);
+        const int per_sm = h->per_sm[ti][h->layout][rate];
         if (cudaStreamWaitEvent(h->rs[rate], h->ev_fork, 0) != cudaSuccess) {
             rc = WLDPC_ERR_CUDA;
             break;
@@ -437,8 +214,6 @@ int wldpc_mixed_create(unsigned max_iter, wldpc_mixed** out)
         cudaGetLastError();
         return WLDPC_ERR_NO_DEVICE;
     }
-    int rc = upload_codes();
-    if (rc) return rc;
     wldpc_mixed* h = new (std::nothrow) wldpc_mixed();
     if (!h) return WLDPC_ERR_ARG;
     h->max_iter = max_iter;
@@ -447,18 +222,20 @@ int wldpc_mixed_create(unsigned max_iter, wldpc_mixed** out)
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev);
     /* shared-memory limit and occupancy of every decode kernel, once, outside any capture */
     for (int ti = 0; ti < 2; ti++)
-        for (int rate = 0; rate < kRates; rate++) {
-            const int T = ti == 0 ? 96 : 192;
-            const MixedKernel k = ti == 0 ? MixedKernels<96>::k[rate] : MixedKernels<192>::k[rate];
-            int per = 0;
-            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, mixed_smem(T)) != cudaSuccess ||
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, T, mixed_smem(T)) != cudaSuccess) {
-                cudaGetLastError();
-                delete h;
-                return WLDPC_ERR_CUDA;
+        for (int layout = 0; layout < 2; layout++)
+            for (int rate = 0; rate < kRates; rate++) {
+                const int T = kThreadChoices[ti];
+                const int smem = mixed_smem_bytes(T, layout);
+                const MixedKernel k = mixed_kernel(ti, layout, rate);
+                int per = 0;
+                if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, T, smem) != cudaSuccess) {
+                    cudaGetLastError();
+                    delete h;
+                    return WLDPC_ERR_CUDA;
+                }
+                h->per_sm[ti][layout][rate] = per > 0 ? per : 1;
             }
-            h->per_sm[ti][rate] = per > 0 ? per : 1;
-        }
     bool ok = true;
     for (int r = 0; r < kRates; r++)
         ok = ok && cudaStreamCreateWithFlags(&h->rs[r], cudaStreamNonBlocking) == cudaSuccess &&
@@ -497,27 +274,44 @@ int wldpc_mixed_destroy(wldpc_mixed* h)
     return WLDPC_OK;
 }
 
-int wldpc_mixed_set_config(wldpc_mixed* h, int threads, int chunk)
+int wldpc_mixed_set_tuning(wldpc_mixed* h, int threads, int layout, int chunk)
 {
-    if (!h || chunk < 1 || chunk > (1 << 20)) return WLDPC_ERR_ARG;
+    if (!h || chunk < 1 || chunk > kMixedMaxChunk) return WLDPC_ERR_ARG;
     if (threads != 96 && threads != 192) return WLDPC_ERR_ARG;
+    if (layout != WLDPC_MIXED_MSG_REGISTERS && layout != WLDPC_MIXED_MSG_SHARED) return WLDPC_ERR_ARG;
     h->threads = threads;
+    h->layout = layout;
     h->chunk = chunk;
     return WLDPC_OK;
 }
 
-int wldpc_mixed_get_config(wldpc_mixed* h, int* threads, int* chunk)
+int wldpc_mixed_get_tuning(wldpc_mixed* h, int* threads, int* layout, int* chunk)
 {
     if (!h) return WLDPC_ERR_ARG;
     if (threads) *threads = h->threads;
+    if (layout) *layout = h->layout;
     if (chunk) *chunk = h->chunk;
     return WLDPC_OK;
+}
+
+int wldpc_mixed_set_config(wldpc_mixed* h, int threads, int chunk)
+{
+    if (!h) return WLDPC_ERR_ARG;
+    return wldpc_mixed_set_tuning(h, threads, h->layout, chunk);
+}
+
+int wldpc_mixed_get_config(wldpc_mixed* h, int* threads, int* chunk)
+{
+    return wldpc_mixed_get_tuning(h, threads, nullptr, chunk);
 }
 
 int wldpc_mixed_decode_device(wldpc_mixed* h, const uint8_t* variant, const int64_t* offset, const float* llr,
                               int8_t* decoded, float* posterior, int32_t* status, size_t frames, void* stream)
 {
     if (!h || (frames && (!variant || !offset || !llr || !decoded))) return WLDPC_ERR_ARG;
+    if (!aligned(llr, 16) || !aligned(decoded, 4) || !aligned(posterior, 16) || !aligned(status, 4) ||
+        !aligned(offset, 8))
+        return WLDPC_ERR_ARG;
     if (frames == 0) return WLDPC_OK;
     if (frames > 0x7fffffff) return WLDPC_ERR_ARG;
     int rc;
@@ -525,7 +319,7 @@ int wldpc_mixed_decode_device(wldpc_mixed* h, const uint8_t* variant, const int6
     if ((rc = h->rank.reserve(frames * sizeof(int))) || (rc = h->perm.reserve(frames * sizeof(int))) ||
         (rc = h->items.reserve(max_items * sizeof(MixedItem))))
         return rc;
-    wldpc_mixed::Key key{variant, offset, llr, decoded, posterior, status, frames, h->threads, h->chunk};
+    wldpc_mixed::Key key{variant, offset, llr, decoded, posterior, status, frames, h->threads, h->layout, h->chunk};
     const cudaStream_t user = (cudaStream_t)stream;
     if (cudaEventRecord(h->ev_in, user) != cudaSuccess || cudaStreamWaitEvent(h->stream, h->ev_in, 0) != cudaSuccess) {
         cudaGetLastError();
@@ -589,45 +383,53 @@ int wldpc_mixed_autotune(wldpc_mixed* h, const uint8_t* variant, const int64_t* 
     if (!h || repeats < 1) return WLDPC_ERR_ARG;
     static const int chunks[4] = {8, 16, 32, 64};
     float best = 1e30f;
-    int bt = h->threads, bc = h->chunk;
+    int bt = h->threads, bl = h->layout, bc = h->chunk;
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         cudaGetLastError();
         return WLDPC_ERR_CUDA;
     }
+    /* CTA size x message layout x frames per work item, timed on the caller's batch */
     for (int ti = 0; ti < 2; ti++)
-        for (int ci = 0; ci < 4; ci++) {
-            h->threads = kThreadChoices[ti];
-            h->chunk = chunks[ci];
-            int rc = wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr, frames, h->stream);
-            if (!rc && cudaEventRecord(e0, h->stream) != cudaSuccess) rc = WLDPC_ERR_CUDA;
-            for (int k = 0; k < repeats && !rc; k++)
-                rc = wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr, frames, h->stream);
-            if (!rc && (cudaEventRecord(e1, h->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
-                rc = WLDPC_ERR_CUDA;
-            if (rc) {
-                cudaGetLastError();
-                cudaEventDestroy(e0);
-                cudaEventDestroy(e1);
-                h->threads = bt;
-                h->chunk = bc;
-                return rc;
+        for (int layout = 0; layout < 2; layout++)
+            for (int ci = 0; ci < 4; ci++) {
+                h->threads = kThreadChoices[ti];
+                h->layout = layout;
+                h->chunk = chunks[ci];
+                int rc = wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr, frames,
+                                                   h->stream);
+                if (!rc && cudaEventRecord(e0, h->stream) != cudaSuccess) rc = WLDPC_ERR_CUDA;
+                for (int k = 0; k < repeats && !rc; k++)
+                    rc = wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr, frames,
+                                                   h->stream);
+                if (!rc && (cudaEventRecord(e1, h->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
+                    rc = WLDPC_ERR_CUDA;
+                if (rc) {
+                    cudaGetLastError();
+                    cudaEventDestroy(e0);
+                    cudaEventDestroy(e1);
+                    h->threads = bt;
+                    h->layout = bl;
+                    h->chunk = bc;
+                    return rc;
+                }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ms /= repeats;
+                if (ms < best) {
+                    best = ms;
+                    bt = h->threads;
+                    bl = h->layout;
+                    bc = h->chunk;
+                }
             }
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            ms /= repeats;
-            if (ms < best) {
-                best = ms;
-                bt = h->threads;
-                bc = h->chunk;
-            }
-        }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     h->threads = bt;
+    h->layout = bl;
     h->chunk = bc;
     if (best_ms) *best_ms = best;
-    return WLDPC_OK;
+    return wldpc_mixed_synchronize(h);
 }
 
 }  // extern "C"

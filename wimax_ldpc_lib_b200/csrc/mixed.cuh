@@ -7,21 +7,19 @@
  *   1. binning (mixed_count / mixed_plan / mixed_scatter): frames are
  *      grouped by code (variant = rate * 19 + z index) and cut into work
  *      items of at most `chunk` frames of one code;
- *   2. mixed_decode_kernel<rate>: one persistent grid per rate, all six
- *      launched concurrently; each CTA takes work items of its rate from that
- *      rate's counter. Within an item the CTA runs G = THREADS / z frame
- *      slots in lockstep (one thread per expanded row, as the specialised
- *      kernel) and refills a slot with the item's next frame as soon as its
- *      frame converges or reaches the cap (early-exit compaction), so no slot
- *      idles while the item has frames left. A refilled frame gets its initial
+ *   2. mixed_decode_kernel<rate, threads, layout> (mixed_kernel.cuh): one
+ *      persistent grid per rate, all six launched concurrently; each CTA
+ *      takes work items of its rate from that rate's counter and decodes an
+ *      item with a body specialised on its z. The CTA runs G = threads / z
+ *      frame slots in lockstep and refills a slot with the item's next frame
+ *      (prefetched by a bulk copy) as soon as its frame converges or reaches
+ *      the cap (early-exit compaction). A refilled frame gets its initial
  *      syndrome check before its first iteration, as in the reference
  *      (reference lib/ldpc_decoder.cc:127-139).
- * Codes are read from a __constant__ table (z, block columns x z, shifts);
- * each rate has its own kernel (one kernel for all six would need the union
- * of their registers), z is a run-time value, and each thread's edge
- * addresses for the current code sit in a shared-memory table. The binning
- * kernels and the six decode kernels (forked onto six streams) are captured
- * in one CUDA graph, so a batch is one graph launch.
+ * The binning kernels and the six decode grids (forked onto six streams) are
+ * captured in one CUDA graph, so a batch is one graph launch. CTA size,
+ * message layout (registers or shared memory) and chunk are picked by the
+ * handle's autotuner.
  */
 #ifndef WLDPC_MIXED_CUH
 #define WLDPC_MIXED_CUH
@@ -34,12 +32,8 @@
 namespace wldpc {
 
 constexpr int kVariants = kRates * kNumZ;   /* 114 */
-
-struct MixedCode {
-    unsigned short z, n;
-    unsigned short colz[96];    /* block column * z, row-major block order */
-    unsigned char shift[96];
-};
+constexpr int kMixedMaxSlots = 8;          /* frames per CTA: 192 threads / z = 24 */
+constexpr int kMixedMaxChunk = 64;         /* frames per work item */
 
 struct MixedItem {
     int variant;
@@ -49,7 +43,7 @@ struct MixedItem {
 
 struct MixedArgs {
     const uint8_t* variant;     /* per frame: rate * 19 + (z - 24) / 4 */
-    const long long* offset;    /* per frame: element offset of its n values */
+    const long long* offset;    /* per frame: element offset of its n values (a multiple of 4) */
     const float* llr;
     int8_t* hard;
     float* post;                /* or null */

@@ -139,6 +139,104 @@ __device__ __forceinline__ float* post_ptr(float* P, float* Pr, float* Prz, int 
 
 __device__ __forceinline__ float canon(float x) { return __fadd_rn(x, 0.0f); }
 
+/* One layer (base row I) of one iteration for the thread's row: pass 1
+ * (L = posterior - old message, sign bits, the two minima), pass 2 (new
+ * messages and posteriors in the mode's arithmetic) and the new compressed
+ * messages M1, M2 (rounded magnitudes) and NEG (sign bit d-1-e of edge e |
+ * argmin edge << 27). at(e) gives the posterior of edge e of this layer for
+ * this row. Used by the specialised decoder and by the mixed-code decoder. */
+template <int R, int I, int MODE, typename At>
+__device__ __forceinline__ void tdmp_layer(At&& at, float& M1, float& M2, uint32_t& NEG)
+{
+    constexpr int d = layer_degree(R, I);
+    float L[d];
+    uint32_t LC[d];
+    uint32_t sgn = 0;
+    float m1, m2;
+    const float oM1 = M1, oM2 = M2;
+    const uint32_t oNeg = NEG;
+    const int oIdx = (int)(oNeg >> 27);
+    /* pass 1: L = post - old message, sign bits, two minima */
+    static_for<d>([&](auto E) {
+        constexpr int e = decltype(E)::value;
+        const float x = *at(E);
+        const float mag = (oIdx == e) ? oM2 : oM1;
+        const uint32_t sb = (oNeg << (32 - d + e)) & 0x80000000u;
+        const float msg = __uint_as_float(__float_as_uint(mag) | sb);
+        const float l = __fsub_rn(x, msg);
+        L[e] = l;
+        LC[e] = __float_as_uint(canon(l));
+        sgn = __funnelshift_l(LC[e], sgn, 1);
+    });
+    two_min_abs<0, d>(L, m1, m2);
+    m1 = fminf(m1, 10000.0f);
+    m2 = fminf(m2, 10000.0f);
+    /* bit (d-1-e) of sgn is neg(L_e); message e is negative iff
+     * (d & 1) ^ parity(neg) ^ neg(L_e)  (reference :148,172,191) */
+    const uint32_t flip = (uint32_t)((d & 1) ^ (__popc(sgn) & 1));
+    const uint32_t dmask = (d >= 32) ? 0xffffffffu : ((1u << d) - 1u);
+    int nIdx = 0;
+    if constexpr (MODE == kMs) {
+        const uint32_t fb = flip << 31;
+        static_for<d>([&](auto E) {
+            constexpr int e = decltype(E)::value;
+            const float l = L[e];
+            const bool is_min = fabsf(l) == m1;
+            const float mu = is_min ? m2 : m1;
+            nIdx = is_min ? e : nIdx;
+            const uint32_t sb = (LC[e] & 0x80000000u) ^ fb;
+            const float t = __uint_as_float(__float_as_uint(mu) | sb);
+            *at(E) = __fadd_rn(l, t);
+        });
+        M1 = m1;
+        M2 = m2;
+    } else {
+        double D1, D2;
+        if constexpr (MODE == kNms) {
+            D1 = __dmul_rn((double)m1, 0.815);
+            D2 = __dmul_rn((double)m2, 0.815);
+        } else {
+            const double t1 = __dsub_rn((double)m1, 0.10);
+            const double t2 = __dsub_rn((double)m2, 0.10);
+            D1 = t1 < 0.0 ? 0.0 : t1;
+            D2 = t2 < 0.0 ? 0.0 : t2;
+        }
+        const uint32_t fb = flip << 31;
+        const int h1 = __double2hiint(D1) ^ (int)fb, l1 = __double2loint(D1);
+        const int h2 = __double2hiint(D2) ^ (int)fb, l2 = __double2loint(D2);
+        static_for<d>([&](auto E) {
+            constexpr int e = decltype(E)::value;
+            const float l = L[e];
+            const bool is_min = fabsf(l) == m1;
+            nIdx = is_min ? e : nIdx;
+            int hi = is_min ? h2 : h1;
+            const int lo = is_min ? l2 : l1;
+            hi ^= (int)(LC[e] & 0x80000000u);
+            const double t = __hiloint2double(hi, lo);
+            *at(E) = __double2float_rn(__dadd_rn((double)l, t));
+        });
+        M1 = __double2float_rn(D1);
+        M2 = __double2float_rn(D2);
+    }
+    NEG = ((sgn ^ (flip ? dmask : 0u)) & dmask) | ((uint32_t)nIdx << 27);
+}
+
+/* Syndrome of the thread's rows over all layers: 1 if any row fails. The
+ * hard decision is x >= 0 (-0.0 is bit 1); a row of degree d fails when d
+ * minus its number of negative posteriors is odd. at(I, E) as in tdmp_layer. */
+template <int R, typename At>
+__device__ __forceinline__ unsigned tdmp_rows_fail(At&& at)
+{
+    unsigned fail = 0;
+    static_for<kMb[R]>([&](auto I) {
+        constexpr int d = layer_degree(R, I);
+        bool odd = (d & 1) != 0;
+        static_for<d>([&](auto E) { odd = odd != (*at(I, E) < 0.0f); });
+        fail |= odd ? 1u : 0u;
+    });
+    return fail;
+}
+
 template <int R, int ZT, int MODE>
 __global__ void __launch_bounds__(TdmpShape<R, ZT>::THREADS)
 tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
@@ -183,16 +281,9 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
 
     /* syndrome of the current posterior for this thread's rows: 1 if any fails */
     auto rows_fail = [&]() -> unsigned {
-        unsigned fail = 0;
-        static_for<MB>([&](auto I) {
-            constexpr int d = layer_degree(R, I);
-            bool odd = (d & 1) != 0;   /* parity of the hard bits: d minus the negatives */
-            static_for<d>([&](auto E) {
-                odd = odd != (*post_ptr<R, ZT, I, E>(P, Pr, Prz, r, a) < 0.0f);
-            });
-            fail |= odd ? 1u : 0u;
+        return tdmp_rows_fail<R>([&](auto I, auto E) {
+            return post_ptr<R, ZT, decltype(I)::value, decltype(E)::value>(P, Pr, Prz, r, a);
         });
-        return fail;
     };
     /* per-frame OR over the CTA; returns this frame's flag and whether any
      * live frame is still failing */
@@ -226,79 +317,10 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
             if (tid == 0) s_fail[it & 1] = 0;   /* slot it&1 was last read before the previous barrier */
         }
         static_for<MB>([&](auto I) {
-            constexpr int d = layer_degree(R, I);
-            if (active) {
-                float L[d];
-                uint32_t LC[d];
-                uint32_t sgn = 0;
-                float m1, m2;
-                const float oM1 = M1[I], oM2 = M2[I];
-                const uint32_t oNeg = NEG[I];
-                const int oIdx = (int)(oNeg >> 27);
-                /* pass 1: L = post - old message, sign bits, two minima */
-                static_for<d>([&](auto E) {
-                    constexpr int e = decltype(E)::value;
-                    const float x = *post_ptr<R, ZT, I, e>(P, Pr, Prz, r, a);
-                    const float mag = (oIdx == e) ? oM2 : oM1;
-                    const uint32_t sb = (oNeg << (32 - d + e)) & 0x80000000u;
-                    const float msg = __uint_as_float(__float_as_uint(mag) | sb);
-                    const float l = __fsub_rn(x, msg);
-                    L[e] = l;
-                    LC[e] = __float_as_uint(canon(l));
-                    sgn = __funnelshift_l(LC[e], sgn, 1);
-                });
-                two_min_abs<0, d>(L, m1, m2);
-                m1 = fminf(m1, 10000.0f);
-                m2 = fminf(m2, 10000.0f);
-                /* bit (d-1-e) of sgn is neg(L_e); message e is negative iff
-                 * (d & 1) ^ parity(neg) ^ neg(L_e)  (reference :148,172,191) */
-                const uint32_t flip = (uint32_t)((d & 1) ^ (__popc(sgn) & 1));
-                const uint32_t dmask = (d >= 32) ? 0xffffffffu : ((1u << d) - 1u);
-                int nIdx = 0;
-                if constexpr (MODE == kMs) {
-                    const uint32_t fb = flip << 31;
-                    static_for<d>([&](auto E) {
-                        constexpr int e = decltype(E)::value;
-                        const float l = L[e];
-                        const bool is_min = fabsf(l) == m1;
-                        const float mu = is_min ? m2 : m1;
-                        nIdx = is_min ? e : nIdx;
-                        const uint32_t sb = (LC[e] & 0x80000000u) ^ fb;
-                        const float t = __uint_as_float(__float_as_uint(mu) | sb);
-                        *post_ptr<R, ZT, I, e>(P, Pr, Prz, r, a) = __fadd_rn(l, t);
-                    });
-                    M1[I] = m1;
-                    M2[I] = m2;
-                } else {
-                    double D1, D2;
-                    if constexpr (MODE == kNms) {
-                        D1 = __dmul_rn((double)m1, 0.815);
-                        D2 = __dmul_rn((double)m2, 0.815);
-                    } else {
-                        const double t1 = __dsub_rn((double)m1, 0.10);
-                        const double t2 = __dsub_rn((double)m2, 0.10);
-                        D1 = t1 < 0.0 ? 0.0 : t1;
-                        D2 = t2 < 0.0 ? 0.0 : t2;
-                    }
-                    const uint32_t fb = flip << 31;
-                    const int h1 = __double2hiint(D1) ^ (int)fb, l1 = __double2loint(D1);
-                    const int h2 = __double2hiint(D2) ^ (int)fb, l2 = __double2loint(D2);
-                    static_for<d>([&](auto E) {
-                        constexpr int e = decltype(E)::value;
-                        const float l = L[e];
-                        const bool is_min = fabsf(l) == m1;
-                        nIdx = is_min ? e : nIdx;
-                        int hi = is_min ? h2 : h1;
-                        const int lo = is_min ? l2 : l1;
-                        hi ^= (int)(LC[e] & 0x80000000u);
-                        const double t = __hiloint2double(hi, lo);
-                        *post_ptr<R, ZT, I, e>(P, Pr, Prz, r, a) = __double2float_rn(__dadd_rn((double)l, t));
-                    });
-                    M1[I] = __double2float_rn(D1);
-                    M2[I] = __double2float_rn(D2);
-                }
-                NEG[I] = ((sgn ^ (flip ? dmask : 0u)) & dmask) | ((uint32_t)nIdx << 27);
-            }
+            if (active)
+                tdmp_layer<R, decltype(I)::value, MODE>(
+                    [&](auto E) { return post_ptr<R, ZT, decltype(I)::value, decltype(E)::value>(P, Pr, Prz, r, a); },
+                    M1[I], M2[I], NEG[I]);
             __syncthreads();
         });
         const bool f = frame_fail(live && active ? rows_fail() : 0u, it & 1, any_fail);

@@ -91,7 +91,7 @@ def main():
     status = torch.empty(args.frames, dtype=torch.int32, device="cuda")
     mixed = wl.MixedDecoder(10)
     best = mixed.autotune(variants, offsets, llr, hard, repeats=3)
-    threads, chunk = mixed.config()
+    threads, layout, chunk = mixed.tuning()
     stream = torch.cuda.Stream()
     for _ in range(3):
         mixed.decode_device(variants, offsets, llr, hard, None, status, stream=stream)
@@ -122,7 +122,8 @@ def main():
     res = {"workload": "mixed batch: code uniform over 114 (rate, z), Eb/N0 U[1, 4] dB, cap 10",
                       "frames": args.frames, "info_bits_per_batch": info_bits,
                       "mixed": {"ms": ms_mixed, "info_gbps": info_bits / (ms_mixed * 1e-3) / 1e9,
-                                "threads": threads, "chunk": chunk, "autotune_best_ms": best},
+                                "threads": threads, "chunk": chunk,
+                                "messages": ["registers", "shared"][layout], "autotune_best_ms": best},
                       "per_code_launches": {"ms": ms_split, "info_gbps": info_bits / (ms_split * 1e-3) / 1e9,
                                             "launches": len(groups)},
                       "bit_exact_match": same_hard and same_status,
