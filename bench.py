@@ -537,7 +537,7 @@ def run_ours(args):
         status_m = torch.empty(MIXED_FRAMES, dtype=torch.int32, device=dev)
         mixed = wl.MixedDecoder(MAX_ITER)
         mixed.autotune(variants, offsets, llr_m, hard_m, repeats=2)
-        threads, layout, chunk = mixed.tuning()
+        threads, layout, chunk, launch = mixed.tuning()
         ms_m = timed_steps(lambda: mixed.decode_device(variants, offsets, llr_m, hard_m, None, status_m,
                                                        stream=stream), args.steps, args.warmup, stream, ws)
         mixed.synchronize()
@@ -550,7 +550,8 @@ def run_ours(args):
                                         "U[1, 4] dB per frame, cap 10, one CUDA-graph launch",
                             "ms_per_step": ms_m, "value": info_bits * ws / (ms_m * 1e-3) / 1e9,
                             "unit": "info Gbit/s", "autotuned": {"threads": threads, "chunk": chunk,
-                                                                "messages": ["registers", "shared"][layout]},
+                                                                "messages": ["registers", "shared"][layout],
+                                                                "launch": ["concurrent", "serial"][launch]},
                             "syndrome_failed_fraction": failed / total, "mean_iterations": iters / total}
         ipf = load_profile_value("mixed_decode_131k.txt", "warp_instructions_per_frame")
         if ipf and clocks.get("sm_mhz"):

@@ -350,16 +350,20 @@ WLDPC_API int wldpc_mixed_synchronize(wldpc_mixed* h);
 /* The autotuner's knobs: CTA size (96 or 192 threads, which sets the frame
  * slots per CTA to threads / z), where each thread's compressed messages
  * live (registers, or shared memory: fewer registers and more resident CTAs)
- * and frames per work item (1..64). set_config / get_config leave the layout
- * as it is. */
+ * frames per work item (1..64) and whether the six per-rate grids run
+ * concurrently or one after another. set_config / get_config leave layout
+ * and launch policy as they are. */
 #define WLDPC_MIXED_MSG_REGISTERS 0
 #define WLDPC_MIXED_MSG_SHARED 1
-WLDPC_API int wldpc_mixed_set_tuning(wldpc_mixed* h, int threads, int layout, int chunk);
-WLDPC_API int wldpc_mixed_get_tuning(wldpc_mixed* h, int* threads, int* layout, int* chunk);
+#define WLDPC_MIXED_CONCURRENT 0
+#define WLDPC_MIXED_SERIAL 1
+WLDPC_API int wldpc_mixed_set_tuning(wldpc_mixed* h, int threads, int layout, int chunk, int launch);
+WLDPC_API int wldpc_mixed_get_tuning(wldpc_mixed* h, int* threads, int* layout, int* chunk, int* launch);
 WLDPC_API int wldpc_mixed_set_config(wldpc_mixed* h, int threads, int chunk);
 WLDPC_API int wldpc_mixed_get_config(wldpc_mixed* h, int* threads, int* chunk);
-/* Times every (threads, layout, chunk) candidate on the given batch (repeats
- * launches each) and keeps the fastest; *best_ms (nullable) gets its time. */
+/* Times every (threads, layout, chunk, launch) candidate on the given batch
+ * (repeats launches each) and keeps the fastest; *best_ms (nullable) gets its
+ * time. */
 WLDPC_API int wldpc_mixed_autotune(wldpc_mixed* h, const uint8_t* variant, const int64_t* offset, const float* llr,
                                    int8_t* decoded, size_t frames, int repeats, float* best_ms);
 

@@ -43,9 +43,11 @@ def test_mixed_matches_specialised_decoders(wl, cuda, batch):
     mixed = wl.MixedDecoder(10)
     R, S = wl.MIXED_MSG_REGISTERS, wl.MIXED_MSG_SHARED
     # every CTA size and message layout; chunks from one frame per item to the maximum
-    for threads, layout, chunk in [(96, R, 32), (96, S, 8), (192, R, 64), (192, S, 16), (96, R, 1), (192, S, 3)]:
-        mixed.set_tuning(threads, layout, chunk)
-        assert mixed.tuning() == (threads, layout, chunk)
+    C, Q = wl.MIXED_CONCURRENT, wl.MIXED_SERIAL
+    for threads, layout, chunk, launch in [(96, R, 32, C), (96, S, 8, Q), (192, R, 64, Q), (192, S, 16, C),
+                                           (96, R, 1, C), (192, S, 3, Q)]:
+        mixed.set_tuning(threads, layout, chunk, launch)
+        assert mixed.tuning() == (threads, layout, chunk, launch)
         for _ in range(2):   # capture, then replay
             hard = torch.zeros(llr.numel(), dtype=torch.int8, device="cuda")
             status = torch.full((frames,), -1, dtype=torch.int32, device="cuda")
@@ -83,8 +85,8 @@ def test_mixed_autotune_and_bad_code(wl, cuda, batch):
     mixed = wl.MixedDecoder(10)
     hard = torch.empty(llr.numel(), dtype=torch.int8, device="cuda")
     ms = mixed.autotune(variants, offsets, llr, hard, repeats=1)
-    threads, layout, chunk = mixed.tuning()
-    assert ms > 0 and threads in (96, 192) and layout in (0, 1) and chunk in (8, 16, 32, 64)
+    threads, layout, chunk, launch = mixed.tuning()
+    assert ms > 0 and threads in (96, 192) and layout in (0, 1) and chunk in (8, 16, 32, 64) and launch in (0, 1)
     bad = variants.clone()
     bad[0] = 200
     mixed.decode_device(bad, offsets, llr, hard)
@@ -102,4 +104,4 @@ def test_mixed_autotune_and_bad_code(wl, cuda, batch):
     mixed.decode_device(variants, offsets, llr, hard)   # and the handle still works
     mixed.synchronize()
     with pytest.raises(wl.LdpcError):
-        mixed.set_tuning(96, 0, 65)                        # at most 64 frames per work item
+        mixed.set_tuning(96, 0, 65, 0)                     # at most 64 frames per work item

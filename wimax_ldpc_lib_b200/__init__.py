@@ -24,6 +24,7 @@ Z_VALUES = tuple(range(24, 97, 4))
 MODE_NMS, MODE_OMS, MODE_MS = 0, 1, 2
 LMS_F32, LMS_F16X2 = 0, 1   # learned-decoder inference arithmetic (wldpc_lms_set_precision)
 MIXED_MSG_REGISTERS, MIXED_MSG_SHARED = 0, 1   # mixed decoder message layout (wldpc_mixed_set_tuning)
+MIXED_CONCURRENT, MIXED_SERIAL = 0, 1           # mixed decoder launch policy of its six per-rate grids
 
 OK = 0
 ERR_ARG, ERR_CODE, ERR_CUDA, ERR_NO_DEVICE, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_SCRATCH = -1, -2, -3, -4, -5, -6, -7
@@ -114,8 +115,9 @@ def _lib():
     L.wldpc_mixed_synchronize.argtypes = [_p]
     L.wldpc_mixed_set_config.argtypes = [_p, _i, _i]
     L.wldpc_mixed_get_config.argtypes = [_p, ctypes.POINTER(_i), ctypes.POINTER(_i)]
-    L.wldpc_mixed_set_tuning.argtypes = [_p, _i, _i, _i]
-    L.wldpc_mixed_get_tuning.argtypes = [_p, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)]
+    L.wldpc_mixed_set_tuning.argtypes = [_p, _i, _i, _i, _i]
+    L.wldpc_mixed_get_tuning.argtypes = [_p, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i),
+                                         ctypes.POINTER(_i)]
     L.wldpc_mixed_autotune.argtypes = [_p, _p, _p, _p, _p, _sz, _i, ctypes.POINTER(ctypes.c_float)]
     L.wldpc_ber_runner_create.argtypes = [_i, _u, _u, _u, ctypes.POINTER(_p)]
     L.wldpc_ber_runner_destroy.argtypes = [_p]
@@ -363,15 +365,17 @@ class MixedDecoder:
         _check(_lib().wldpc_mixed_get_config(self._h, ctypes.byref(t), ctypes.byref(c)), "mixed config")
         return t.value, c.value
 
-    def set_tuning(self, threads: int, layout: int, chunk: int):
-        """CTA size (96 | 192), message layout (MIXED_MSG_*) and frames per work item (1..64)."""
-        _check(_lib().wldpc_mixed_set_tuning(self._h, threads, layout, chunk), "mixed tuning")
+    def set_tuning(self, threads: int, layout: int, chunk: int, launch: int = MIXED_CONCURRENT):
+        """CTA size (96 | 192), message layout (MIXED_MSG_*), frames per work
+        item (1..64) and launch policy (MIXED_CONCURRENT | MIXED_SERIAL)."""
+        _check(_lib().wldpc_mixed_set_tuning(self._h, threads, layout, chunk, launch), "mixed tuning")
 
     def tuning(self):
-        t, l, c = _i(), _i(), _i()
-        _check(_lib().wldpc_mixed_get_tuning(self._h, ctypes.byref(t), ctypes.byref(l), ctypes.byref(c)),
-               "mixed tuning")
-        return t.value, l.value, c.value
+        """(threads, layout, chunk, launch)"""
+        t, l, c, p = _i(), _i(), _i(), _i()
+        _check(_lib().wldpc_mixed_get_tuning(self._h, ctypes.byref(t), ctypes.byref(l), ctypes.byref(c),
+                                             ctypes.byref(p)), "mixed tuning")
+        return t.value, l.value, c.value, p.value
 
     def autotune(self, variants, offsets, llr, decoded, repeats: int = 3) -> float:
         ms = ctypes.c_float()

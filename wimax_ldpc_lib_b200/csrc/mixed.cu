@@ -124,6 +124,7 @@ static MixedKernel mixed_kernel(int ti, int layout, int rate)
 struct wldpc_mixed {
     unsigned max_iter;
     int threads = 192, layout = kMsgShared, chunk = 16;
+    int launch = WLDPC_MIXED_CONCURRENT;   /* the six rate grids: concurrent or one after another */
     int sms = 148;
     int per_sm[2][2][kRates] = {};   /* resident CTAs per SM, [96 | 192 threads][layout][rate] */
     cudaStream_t stream = nullptr;
@@ -137,7 +138,7 @@ struct wldpc_mixed {
     struct Key {
         const void *variant, *offset, *llr, *hard, *post, *status;
         size_t frames;
-        int threads, layout, chunk;
+        int threads, layout, chunk, launch;
         bool operator==(const Key& o) const { return memcmp(this, &o, sizeof(Key)) == 0; }
     } key{};
 };
@@ -173,8 +174,17 @@ static int mixed_enqueue(wldpc_mixed* h, const uint8_t* variant, const long long
     const int T = h->threads;
     const int ti = T == 96 ? 0 : 1;
     const int smem = mixed_smem_bytes(T, h->layout);
+    if (cudaGetLastError() != cudaSuccess) return WLDPC_ERR_CUDA;
+    if (h->launch == WLDPC_MIXED_SERIAL) {
+        /* one rate after another on st, each grid with the whole GPU */
+        for (int rate = 0; rate < kRates; rate++) {
+            mixed_kernel(ti, h->layout, rate)<<<h->sms * h->per_sm[ti][h->layout][rate], T, smem, st>>>(a);
+            if (cudaGetLastError() != cudaSuccess) return WLDPC_ERR_CUDA;
+        }
+        return WLDPC_OK;
+    }
     /* fork: the six rate kernels run concurrently, then join back on st */
-    if (cudaGetLastError() != cudaSuccess || cudaEventRecord(h->ev_fork, st) != cudaSuccess) return WLDPC_ERR_CUDA;
+    if (cudaEventRecord(h->ev_fork, st) != cudaSuccess) return WLDPC_ERR_CUDA;
     /* every forked stream is joined back even when a step fails, so that a
      * capture in progress always ends with all its streams joined */
     int rc = WLDPC_OK;
@@ -274,35 +284,38 @@ int wldpc_mixed_destroy(wldpc_mixed* h)
     return WLDPC_OK;
 }
 
-int wldpc_mixed_set_tuning(wldpc_mixed* h, int threads, int layout, int chunk)
+int wldpc_mixed_set_tuning(wldpc_mixed* h, int threads, int layout, int chunk, int launch)
 {
     if (!h || chunk < 1 || chunk > kMixedMaxChunk) return WLDPC_ERR_ARG;
     if (threads != 96 && threads != 192) return WLDPC_ERR_ARG;
     if (layout != WLDPC_MIXED_MSG_REGISTERS && layout != WLDPC_MIXED_MSG_SHARED) return WLDPC_ERR_ARG;
+    if (launch != WLDPC_MIXED_CONCURRENT && launch != WLDPC_MIXED_SERIAL) return WLDPC_ERR_ARG;
     h->threads = threads;
     h->layout = layout;
     h->chunk = chunk;
+    h->launch = launch;
     return WLDPC_OK;
 }
 
-int wldpc_mixed_get_tuning(wldpc_mixed* h, int* threads, int* layout, int* chunk)
+int wldpc_mixed_get_tuning(wldpc_mixed* h, int* threads, int* layout, int* chunk, int* launch)
 {
     if (!h) return WLDPC_ERR_ARG;
     if (threads) *threads = h->threads;
     if (layout) *layout = h->layout;
     if (chunk) *chunk = h->chunk;
+    if (launch) *launch = h->launch;
     return WLDPC_OK;
 }
 
 int wldpc_mixed_set_config(wldpc_mixed* h, int threads, int chunk)
 {
     if (!h) return WLDPC_ERR_ARG;
-    return wldpc_mixed_set_tuning(h, threads, h->layout, chunk);
+    return wldpc_mixed_set_tuning(h, threads, h->layout, chunk, h->launch);
 }
 
 int wldpc_mixed_get_config(wldpc_mixed* h, int* threads, int* chunk)
 {
-    return wldpc_mixed_get_tuning(h, threads, nullptr, chunk);
+    return wldpc_mixed_get_tuning(h, threads, nullptr, chunk, nullptr);
 }
 
 int wldpc_mixed_decode_device(wldpc_mixed* h, const uint8_t* variant, const int64_t* offset, const float* llr,
@@ -319,7 +332,8 @@ int wldpc_mixed_decode_device(wldpc_mixed* h, const uint8_t* variant, const int6
     if ((rc = h->rank.reserve(frames * sizeof(int))) || (rc = h->perm.reserve(frames * sizeof(int))) ||
         (rc = h->items.reserve(max_items * sizeof(MixedItem))))
         return rc;
-    wldpc_mixed::Key key{variant, offset, llr, decoded, posterior, status, frames, h->threads, h->layout, h->chunk};
+    wldpc_mixed::Key key{variant,  offset,     llr,       decoded,  posterior, status,
+                         frames,   h->threads, h->layout, h->chunk, h->launch};
     const cudaStream_t user = (cudaStream_t)stream;
     if (cudaEventRecord(h->ev_in, user) != cudaSuccess || cudaStreamWaitEvent(h->stream, h->ev_in, 0) != cudaSuccess) {
         cudaGetLastError();
@@ -383,19 +397,22 @@ int wldpc_mixed_autotune(wldpc_mixed* h, const uint8_t* variant, const int64_t* 
     if (!h || repeats < 1) return WLDPC_ERR_ARG;
     static const int chunks[4] = {8, 16, 32, 64};
     float best = 1e30f;
-    int bt = h->threads, bl = h->layout, bc = h->chunk;
+    int bt = h->threads, bl = h->layout, bc = h->chunk, bp = h->launch;
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         cudaGetLastError();
         return WLDPC_ERR_CUDA;
     }
-    /* CTA size x message layout x frames per work item, timed on the caller's batch */
+    /* CTA size x message layout x frames per work item x launch policy, timed
+     * on the caller's batch */
     for (int ti = 0; ti < 2; ti++)
         for (int layout = 0; layout < 2; layout++)
-            for (int ci = 0; ci < 4; ci++) {
+            for (int ci = 0; ci < 4; ci++)
+                for (int lp = 0; lp < 2; lp++) {
                 h->threads = kThreadChoices[ti];
                 h->layout = layout;
                 h->chunk = chunks[ci];
+                h->launch = lp;
                 int rc = wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr, frames,
                                                    h->stream);
                 if (!rc && cudaEventRecord(e0, h->stream) != cudaSuccess) rc = WLDPC_ERR_CUDA;
@@ -411,6 +428,7 @@ int wldpc_mixed_autotune(wldpc_mixed* h, const uint8_t* variant, const int64_t* 
                     h->threads = bt;
                     h->layout = bl;
                     h->chunk = bc;
+                    h->launch = bp;
                     return rc;
                 }
                 float ms = 0.f;
@@ -421,13 +439,15 @@ int wldpc_mixed_autotune(wldpc_mixed* h, const uint8_t* variant, const int64_t* 
                     bt = h->threads;
                     bl = h->layout;
                     bc = h->chunk;
+                    bp = h->launch;
                 }
-            }
+                }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     h->threads = bt;
     h->layout = bl;
     h->chunk = bc;
+    h->launch = bp;
     if (best_ms) *best_ms = best;
     return wldpc_mixed_synchronize(h);
 }

@@ -18,7 +18,10 @@
  * LAYOUT selects where a thread's compressed messages (M1, M2, NEG per
  * layer) live: in registers, or in shared memory (fewer registers, more
  * resident CTAs). The arithmetic is the plain normalized min-sum of
- * tdmp_layer(), bit-exact with the reference.
+ * tdmp_layer(), bit-exact with the reference. The six per-rate grids run
+ * concurrently or one after another (the handle's launch policy): together
+ * they fill each other's stalls, one at a time they keep fewer z bodies in
+ * the instruction caches.
  *
  * Every mbarrier wait is bounded: on expiry the kernel records
  * kErrWaitTimeout, waits (bounded) for the copies it has in flight and exits.
@@ -64,10 +67,23 @@ struct MixedCtl {
     int item;
 };
 
+/* The CTA's shared state, at file scope so that the z bodies, which are not
+ * inlined, still address it as shared memory: the posterior buffers (and the
+ * shared-layout messages) in the dynamic shared memory, the control block and
+ * one mbarrier per (buffer, slot). */
+extern __shared__ __align__(128) float g_mixed_smem[];
+static __shared__ MixedCtl g_mixed_ctl;
+static __shared__ __align__(8) uint64_t g_mixed_bar[2][kMixedMaxSlots];
+
+/* Not inlined: each z body gets its own register allocation (with all 19
+ * inlined into one kernel the register layout's messages went to local
+ * memory); the call happens once per work item. */
 template <int R, int Z, int THREADS, int LAYOUT>
-__device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem item, float* smem,
-                                           uint64_t (*bar)[kMixedMaxSlots], MixedCtl& S)
+__device__ __noinline__ bool mixed_item(const MixedArgs& a, const MixedItem item)
 {
+    float* const smem = g_mixed_smem;
+    MixedCtl& S = g_mixed_ctl;
+    auto& bar = g_mixed_bar;
     constexpr int MB = kMb[R];
     constexpr int N = kNB * Z;
     constexpr int G = THREADS / Z;
@@ -256,12 +272,10 @@ template <int R, int THREADS, int LAYOUT>
 __global__ void __launch_bounds__(THREADS, (MixedOcc<THREADS, LAYOUT>::MIN_CTAS))
 mixed_decode_kernel(const __grid_constant__ MixedArgs a)
 {
-    extern __shared__ __align__(128) float smem_mixed[];
-    __shared__ __align__(8) uint64_t bar[2][kMixedMaxSlots];
-    __shared__ MixedCtl S;
+    MixedCtl& S = g_mixed_ctl;
     if (threadIdx.x == 0) {
         for (int b = 0; b < 2; b++)
-            for (int q = 0; q < kMixedMaxSlots; q++) mbar_init(&bar[b][q], 1);
+            for (int q = 0; q < kMixedMaxSlots; q++) mbar_init(&g_mixed_bar[b][q], 1);
         fence_mbar_init();
         S.cur = 0xffffffffu;     /* first frames go into buffer 0 */
         S.phase = 0;
@@ -278,7 +292,7 @@ mixed_decode_kernel(const __grid_constant__ MixedArgs a)
         bool ok = true;
         static_for<kNumZ>([&](auto ZI) {
             constexpr int zi_c = decltype(ZI)::value;
-            if (zi == zi_c) ok = mixed_item<R, kZMin + kZStep * zi_c, THREADS, LAYOUT>(a, it, smem_mixed, bar, S);
+            if (zi == zi_c) ok = mixed_item<R, kZMin + kZStep * zi_c, THREADS, LAYOUT>(a, it);
         });
         if (!ok) break;
         __syncthreads();

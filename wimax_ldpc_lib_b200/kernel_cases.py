@@ -1,7 +1,14 @@
-"""Runs each kernel of the library on one seeded case of a chosen size, for
-profilers (ncu) and quick timing: the kernels outside bench.py's workload.
+"""Runs each kernel of the library once on one seeded case of a chosen size,
+for profilers (ncu: every launch below is one capture) and quick timing.
 
-  python -m wimax_ldpc_lib_b200.kernel_cases [--frames F] [--cases train,syndrome,bits,lfsr,nullspace]
+  python -m wimax_ldpc_lib_b200.kernel_cases [--frames F] [--cases decode,encode,train,syndrome,bits,lfsr,nullspace]
+
+  decode     F frames of rate 1/2 z = 96 at 2.25 dB and of rate 5/6 z = 96 at
+             4 dB (framegen_kernel), each decoded once by the plain decoder
+             (tdmp_decode_kernel), the learned decoder with its shipped
+             weights (lms_decode_kernel) and the same weights in packed
+             binary16 (lms16_decode_kernel), cap 10
+  encode     F rate 1/2 z = 96 info words (encode_bytes_kernel)
 
   train      one Adam step of the learned decoder's training (rate 1/2,
              z = 96, F/16 frames generated on the device): framegen_kernel,
@@ -32,7 +39,7 @@ sys.path.insert(0, os.path.dirname(HERE))
 
 import wimax_ldpc_lib_b200 as wl  # noqa: E402
 
-CASES = ("train", "syndrome", "bits", "lfsr", "nullspace")
+CASES = ("decode", "encode", "train", "syndrome", "bits", "lfsr", "nullspace")
 
 
 def main():
@@ -47,7 +54,31 @@ def main():
     rng = np.random.default_rng(args.seed)
     for case in [c for c in args.cases.split(",") if c]:
         t0 = time.perf_counter()
-        if case == "train":
+        if case == "decode":
+            extra = []
+            for rate, ebno in ((0, 2.25), (5, 4.0)):
+                n = 24 * 96
+                llr = torch.empty((F, n), dtype=torch.float32, device="cuda")
+                hard = torch.empty((F, n), dtype=torch.int8, device="cuda")
+                st = torch.empty(F, dtype=torch.int32, device="cuda")
+                wl.framegen_device(rate, 96, args.seed, 0, F, ebno, ebno, llr=llr)
+                meta, w, _ = wl.learned_weights(rate, 96)
+                decs = [wl.Decoder(rate, 96, 10),
+                        wl.LearnedDecoder(rate, 96, meta["iterations"], weights=w, cap=10),
+                        wl.LearnedDecoder(rate, 96, meta["iterations"], weights=w, cap=10, precision=wl.LMS_F16X2)]
+                for dec in decs:
+                    dec.decode_device(llr, hard, None, st)
+                    torch.cuda.synchronize()
+                    extra.append(f"{(st & 0xFFFF).float().mean().item():.2f}")
+            extra = "mean iterations " + " ".join(extra)
+        elif case == "encode":
+            enc = wl.Encoder(0, 96)
+            info = torch.from_numpy(rng.integers(0, 2, (F, enc.k), dtype=np.uint8)).cuda()
+            cw = torch.empty((F, enc.n), dtype=torch.uint8, device="cuda")
+            enc.encode_device(info, cw)
+            torch.cuda.synchronize()
+            extra = f"codeword weight {cw.float().mean().item():.3f}"
+        elif case == "train":
             lms = wl.LearnedDecoder(0, 96, 8)
             hist = lms.train(1, max(64, F // 16), 1.0, 3.0, args.seed)
             extra = f"loss {hist[0]:.5f}"

@@ -1,6 +1,6 @@
 """Mixed-code batches: building them on the device, and the mixed-batch benchmark.
 
-  python -m wimax_ldpc_lib_b200.mixed_batch [--frames 131072] [--steps 10]
+  python -m wimax_ldpc_lib_b200.mixed_batch [--frames 131072] [--steps 10] [--sweep] [--tuning T,L,C,P]
 
 The workload draws every frame's code uniformly over the 114 (rate, z) codes
 and its Eb/N0 uniformly in [1, 4] dB; rate 3/4B frames are random codewords
@@ -9,7 +9,11 @@ from the encoder. Frames are stored back to back (frame f at offset[f]) and
 presented to the decoder in a random order. The benchmark autotunes the
 persistent decoder, times one-graph-launch decodes with CUDA events, and
 times the same frames decoded code by code with the (rate, z)-specialised
-kernels for comparison; both must agree bit for bit.
+kernels for comparison; both must agree bit for bit. --sweep also times every
+candidate of the autotuner's space (CTA threads x message layout x chunk x
+launch policy) and reports the table; --tuning T,L,C,P skips the autotuner
+and uses that candidate (threads, layout 0 = registers / 1 = shared, chunk,
+launch 0 = concurrent / 1 = serial).
 """
 from __future__ import annotations
 
@@ -85,14 +89,41 @@ def main():
     ap.add_argument("--frames", type=int, default=131072)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--out", default=None, help="also write the JSON result to this file")
+    ap.add_argument("--sweep", action="store_true", help="time every tuning candidate")
+    ap.add_argument("--tuning", default=None, help="threads,layout,chunk,launch instead of the autotuner")
     args = ap.parse_args()
     variants, offsets, llr, cw, groups = build_batch(args.frames)
     hard = torch.empty(llr.numel(), dtype=torch.int8, device="cuda")
     status = torch.empty(args.frames, dtype=torch.int32, device="cuda")
     mixed = wl.MixedDecoder(10)
-    best = mixed.autotune(variants, offsets, llr, hard, repeats=3)
-    threads, layout, chunk = mixed.tuning()
     stream = torch.cuda.Stream()
+    table = []
+    if args.sweep:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for threads in (96, 192):
+            for layout in (wl.MIXED_MSG_REGISTERS, wl.MIXED_MSG_SHARED):
+                for chunk in (8, 16, 32, 64):
+                    for launch in (wl.MIXED_CONCURRENT, wl.MIXED_SERIAL):
+                        mixed.set_tuning(threads, layout, chunk, launch)
+                        mixed.decode_device(variants, offsets, llr, hard, None, status, stream=stream)
+                        e0.record(stream)
+                        for _ in range(3):
+                            mixed.decode_device(variants, offsets, llr, hard, None, status, stream=stream)
+                        e1.record(stream)
+                        torch.cuda.synchronize()
+                        mixed.synchronize()
+                        ms = e0.elapsed_time(e1) / 3
+                        table.append({"threads": threads, "messages": ["registers", "shared"][layout], "chunk": chunk,
+                                      "launch": ["concurrent", "serial"][launch], "ms": ms})
+                        print(f"sweep: {threads:3d} threads, messages in {table[-1]['messages']:9s}, chunk {chunk:2d}, "
+                              f"{table[-1]['launch']:10s}: {ms:7.3f} ms")
+    if args.tuning:
+        t, l, c, p = (int(x) for x in args.tuning.split(","))
+        mixed.set_tuning(t, l, c, p)
+        best = None
+    else:
+        best = mixed.autotune(variants, offsets, llr, hard, repeats=3)
+    threads, layout, chunk, launch = mixed.tuning()
     for _ in range(3):
         mixed.decode_device(variants, offsets, llr, hard, None, status, stream=stream)
     torch.cuda.synchronize()
@@ -122,14 +153,14 @@ def main():
     res = {"workload": "mixed batch: code uniform over 114 (rate, z), Eb/N0 U[1, 4] dB, cap 10",
                       "frames": args.frames, "info_bits_per_batch": info_bits,
                       "mixed": {"ms": ms_mixed, "info_gbps": info_bits / (ms_mixed * 1e-3) / 1e9,
-                                "threads": threads, "chunk": chunk,
-                                "messages": ["registers", "shared"][layout], "autotune_best_ms": best},
+                                "threads": threads, "chunk": chunk, "messages": ["registers", "shared"][layout],
+                                "launch": ["concurrent", "serial"][launch], "autotune_best_ms": best},
                       "per_code_launches": {"ms": ms_split, "info_gbps": info_bits / (ms_split * 1e-3) / 1e9,
                                             "launches": len(groups)},
                       "bit_exact_match": same_hard and same_status,
                       "hard_bits_match": same_hard, "status_match": same_status, "syndrome_failed_fraction": fer_frames,
                       "mean_iterations": float((status & 0xFFFF).double().mean().item()),
-                      "device": torch.cuda.get_device_name(0)}
+                      "device": torch.cuda.get_device_name(0), "sweep": table}
     print(json.dumps(res))
     if args.out:
         os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
