@@ -91,8 +91,11 @@ def main():
     ap.add_argument("--out", default=None, help="also write the JSON result to this file")
     ap.add_argument("--sweep", action="store_true", help="time every tuning candidate")
     ap.add_argument("--tuning", default=None, help="threads,layout,chunk,launch instead of the autotuner")
+    ap.add_argument("--z", type=int, nargs="*", default=None, help="only these z values")
+    ap.add_argument("--rates", type=int, nargs="*", default=None, help="only these rates")
     args = ap.parse_args()
-    variants, offsets, llr, cw, groups = build_batch(args.frames)
+    codes = [(r, z) for r in (args.rates if args.rates else range(6)) for z in (args.z if args.z else wl.Z_VALUES)]
+    variants, offsets, llr, cw, groups = build_batch(args.frames, codes=codes)
     hard = torch.empty(llr.numel(), dtype=torch.int8, device="cuda")
     status = torch.empty(args.frames, dtype=torch.int32, device="cuda")
     mixed = wl.MixedDecoder(10)
@@ -150,7 +153,7 @@ def main():
     same_status = bool(torch.equal(status, status_ref))
     info_bits = sum(c * (24 - [12, 8, 8, 6, 6, 4][r]) * z for (r, z), (_, _, c) in groups.items())
     fer_frames = float(((status >> 16) & 1).double().mean().item())
-    res = {"workload": "mixed batch: code uniform over 114 (rate, z), Eb/N0 U[1, 4] dB, cap 10",
+    res = {"workload": f"mixed batch: code uniform over {len(codes)} (rate, z), Eb/N0 U[1, 4] dB, cap 10",
                       "frames": args.frames, "info_bits_per_batch": info_bits,
                       "mixed": {"ms": ms_mixed, "info_gbps": info_bits / (ms_mixed * 1e-3) / 1e9,
                                 "threads": threads, "chunk": chunk, "messages": ["registers", "shared"][layout],
