@@ -123,8 +123,9 @@ static MixedKernel mixed_kernel(int ti, int layout, int rate)
 
 struct wldpc_mixed {
     unsigned max_iter;
-    int threads = 192, layout = kMsgShared, chunk = 16;
+    int threads = 96, layout = kMsgRegisters, chunk = 16;
     int launch = WLDPC_MIXED_CONCURRENT;   /* the six rate grids: concurrent or one after another */
+    MixedCode codes[kVariants];            /* every code, by variant */
     int sms = 148;
     int per_sm[2][2][kRates] = {};   /* resident CTAs per SM, [96 | 192 threads][layout][rate] */
     cudaStream_t stream = nullptr;
@@ -178,6 +179,7 @@ static int mixed_enqueue(wldpc_mixed* h, const uint8_t* variant, const long long
     if (h->launch == WLDPC_MIXED_SERIAL) {
         /* one rate after another on st, each grid with the whole GPU */
         for (int rate = 0; rate < kRates; rate++) {
+            memcpy(a.codes, h->codes + rate * kNumZ, sizeof(a.codes));
             mixed_kernel(ti, h->layout, rate)<<<h->sms * h->per_sm[ti][h->layout][rate], T, smem, st>>>(a);
             if (cudaGetLastError() != cudaSuccess) return WLDPC_ERR_CUDA;
         }
@@ -195,6 +197,7 @@ static int mixed_enqueue(wldpc_mixed* h, const uint8_t* variant, const long long
             rc = WLDPC_ERR_CUDA;
             break;
         }
+        memcpy(a.codes, h->codes + rate * kNumZ, sizeof(a.codes));
         k<<<h->sms * per_sm, T, smem, h->rs[rate]>>>(a);
         if (cudaGetLastError() != cudaSuccess) rc = WLDPC_ERR_CUDA;
         if (cudaEventRecord(h->ev_join[rate], h->rs[rate]) != cudaSuccess ||
@@ -227,6 +230,19 @@ int wldpc_mixed_create(unsigned max_iter, wldpc_mixed** out)
     wldpc_mixed* h = new (std::nothrow) wldpc_mixed();
     if (!h) return WLDPC_ERR_ARG;
     h->max_iter = max_iter;
+    for (int rate = 0; rate < kRates; rate++)
+        for (int zi = 0; zi < kNumZ; zi++) {
+            const int z = kZMin + kZStep * zi;
+            const CodeDesc c = make_code_desc(rate, z);
+            MixedCode& m = h->codes[rate * kNumZ + zi];
+            memset(&m, 0, sizeof(m));
+            m.z = (unsigned short)z;
+            m.n = (unsigned short)c.n;
+            for (int b = 0; b < c.nblk; b++) {
+                m.colz[b] = (unsigned short)(c.col[b] * z);
+                m.shift[b] = (unsigned char)c.shift[b];
+            }
+        }
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, dev);

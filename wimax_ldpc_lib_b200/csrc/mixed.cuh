@@ -8,14 +8,14 @@
  *      grouped by code (variant = rate * 19 + z index) and cut into work
  *      items of at most `chunk` frames of one code;
  *   2. mixed_decode_kernel<rate, threads, layout> (mixed_kernel.cuh): one
- *      persistent grid per rate, all six launched concurrently; each CTA
- *      takes work items of its rate from that rate's counter and decodes an
- *      item with a body specialised on its z. The CTA runs G = threads / z
- *      frame slots in lockstep and refills a slot with the item's next frame
- *      (prefetched by a bulk copy) as soon as its frame converges or reaches
- *      the cap (early-exit compaction). A refilled frame gets its initial
- *      syndrome check before its first iteration, as in the reference
- *      (reference lib/ldpc_decoder.cc:127-139).
+ *      persistent grid per rate, the six launched concurrently or one after
+ *      another; each CTA takes work items of its rate from that rate's
+ *      counter. The CTA runs G = threads / z frame slots in lockstep (z a
+ *      run-time value, edge addresses from a per-item shared-memory table)
+ *      and refills a slot with the item's next frame (one bulk copy) as soon
+ *      as its frame converges or reaches the cap (early-exit compaction). A
+ *      refilled frame gets its initial syndrome check before its first
+ *      iteration, as in the reference (reference lib/ldpc_decoder.cc:127-139).
  * The binning kernels and the six decode grids (forked onto six streams) are
  * captured in one CUDA graph, so a batch is one graph launch. CTA size,
  * message layout (registers or shared memory) and chunk are picked by the
@@ -34,6 +34,13 @@ namespace wldpc {
 constexpr int kVariants = kRates * kNumZ;   /* 114 */
 constexpr int kMixedMaxSlots = 8;          /* frames per CTA: 192 threads / z = 24 */
 constexpr int kMixedMaxChunk = 64;         /* frames per work item */
+
+/* one code of a rate, as the mixed kernel needs it (z at run time) */
+struct MixedCode {
+    unsigned short z, n;
+    unsigned short colz[96];    /* block column * z, row-major block order */
+    unsigned char shift[96];
+};
 
 struct MixedItem {
     int variant;
@@ -56,6 +63,7 @@ struct MixedArgs {
     unsigned* err;
     long long frames;
     int max_iter;
+    MixedCode codes[kNumZ];     /* the launched rate's 19 codes, by z index */
 };
 
 }  // namespace wldpc

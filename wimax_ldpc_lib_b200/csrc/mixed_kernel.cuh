@@ -1,27 +1,25 @@
 /*
  * The persistent mixed-code decode kernel (mixed.cuh): one grid per code
  * rate takes work items (up to `chunk` frames of one (rate, z)) from its
- * rate's queue and decodes each with a body specialised on z, so every edge
- * address is a compile-time constant as in the specialised decoder
- * (nms_decode.cuh) and no address table is needed.
+ * rate's queue. z is a run-time value, so one kernel body serves all 19 z of
+ * its rate: every thread's edge addresses for the item's code go into a
+ * shared-memory table once per item (one 16-bit load per edge afterwards).
+ * A body specialised on z per item kept every address a compile-time
+ * constant, but 19 such bodies per kernel overflowed the instruction caches
+ * (ncu: 10 no_instruction stalls per issue, issue 16% active) and ran 1.7x
+ * slower on the mixed batch.
  *
  * Within an item the CTA runs G = THREADS / z frame slots in lockstep, one
- * thread per expanded row. Every slot owns two posterior buffers in shared
- * memory: while it decodes the frame in one, the next frame of the item is
- * already on its way into the other by a cp.async.bulk copy (TMA, no
- * multicast) completed on that buffer's mbarrier. When a slot's frame
- * converges or reaches the cap, its outputs are written, the prefetched
- * frame becomes current after its initial syndrome check (reference
- * lib/ldpc_decoder.cc:127-139) and the following frame is fetched into the
- * freed buffer (early-exit compaction without a load on the critical path).
+ * thread per expanded row, and refills a slot as soon as its frame converges
+ * or reaches the cap (early-exit compaction). A refilled frame arrives by one
+ * cp.async.bulk copy (TMA, no multicast) completed on the slot's mbarrier,
+ * and gets its initial syndrome check before its first iteration (reference
+ * lib/ldpc_decoder.cc:127-139). The item's frame list and offsets are staged
+ * in shared memory at its start, so a refill reads no global memory.
  *
  * LAYOUT selects where a thread's compressed messages (M1, M2, NEG per
- * layer) live: in registers, or in shared memory (fewer registers, more
- * resident CTAs). The arithmetic is the plain normalized min-sum of
- * tdmp_layer(), bit-exact with the reference. The six per-rate grids run
- * concurrently or one after another (the handle's launch policy): together
- * they fill each other's stalls, one at a time they keep fewer z bodies in
- * the instruction caches.
+ * layer) live: in registers, or in shared memory. The arithmetic is the
+ * plain normalized min-sum of tdmp_layer(), bit-exact with the reference.
  *
  * Every mbarrier wait is bounded: on expiry the kernel records
  * kErrWaitTimeout, waits (bounded) for the copies it has in flight and exits.
@@ -37,138 +35,105 @@ enum MixedLayout : int { kMsgRegisters = 0, kMsgShared = 1 };
 
 using MixedKernel = void (*)(const MixedArgs);
 
-/* resident CTAs per SM the register allocation is sized for. The register
- * file is split over the SM's four schedulers, so w warps per SM leave
- * 16384 / ceil(w / 4) / 32 registers per thread: with the messages in
- * registers the kernel needs more than 96 (15 warps: 128; 12 warps: 168),
- * with them in shared memory 80 suffice (24 warps). */
-template <int THREADS, int LAYOUT>
+/* resident CTAs per SM the register allocation is sized for (80 registers
+ * per thread; the kernel is latency-bound, so resident warps pay more than
+ * the few spills of the rate-5/6 kernel cost) */
+template <int THREADS>
 struct MixedOcc {
-    static constexpr int MIN_CTAS = LAYOUT == kMsgRegisters ? (THREADS == 96 ? 5 : 2) : (THREADS == 96 ? 8 : 4);
+    static constexpr int MIN_CTAS = THREADS == 96 ? 8 : 4;
 };
 
-/* dynamic shared memory of a CTA: two posterior buffers of 24 floats per
- * thread, plus the messages (3 words per layer per thread) in the shared layout */
+/* dynamic shared memory of a CTA: the posteriors (24 floats per thread), the
+ * 16-bit address table (96 blocks per thread) and, in the shared layout, the
+ * messages (3 words per layer per thread) */
 constexpr int mixed_smem_bytes(int threads, int layout)
 {
-    return 2 * 24 * threads * 4 + (layout == kMsgShared ? 3 * kMaxMb * threads * 4 : 0);
+    return 24 * threads * 4 + 96 * threads * 2 + (layout == kMsgShared ? 3 * kMaxMb * threads * 4 : 0);
 }
 
 struct MixedCtl {
     int flist[kMixedMaxChunk];       /* the item's frames, in decode order */
     long long olist[kMixedMaxChunk]; /* and their LLR offsets */
-    int frame[kMixedMaxSlots];       /* current frame of each slot, -1 = empty */
-    int pre[kMixedMaxSlots];         /* frame prefetched into the other buffer, -1 = none */
-    long long off_cur[kMixedMaxSlots], off_pre[kMixedMaxSlots];
-    unsigned cur;                    /* bit q: buffer holding slot q's current frame */
-    unsigned phase;                  /* bit 8b + q: parity the next wait on bar[b][q] expects */
+    int frame[kMixedMaxSlots];       /* frame of each slot, -1 = empty */
+    long long off[kMixedMaxSlots];
+    unsigned phase;                  /* bit q: parity the next wait on bar[q] expects */
     unsigned fresh, fail, abort;
     int next;                        /* frames of the item handed out */
     int item;
 };
 
-/* The CTA's shared state, at file scope so that the z bodies, which are not
- * inlined, still address it as shared memory: the posterior buffers (and the
- * shared-layout messages) in the dynamic shared memory, the control block and
- * one mbarrier per (buffer, slot). */
-extern __shared__ __align__(128) float g_mixed_smem[];
-static __shared__ MixedCtl g_mixed_ctl;
-static __shared__ __align__(8) uint64_t g_mixed_bar[2][kMixedMaxSlots];
-
-/* Not inlined: each z body gets its own register allocation (with all 19
- * inlined into one kernel the register layout's messages went to local
- * memory); the call happens once per work item. */
-template <int R, int Z, int THREADS, int LAYOUT>
-__device__ __noinline__ bool mixed_item(const MixedArgs& a, const MixedItem item)
+template <int R, int THREADS, int LAYOUT>
+__device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem item, float* smem, MixedCtl& S,
+                                           uint64_t* bar)
 {
-    float* const smem = g_mixed_smem;
-    MixedCtl& S = g_mixed_ctl;
-    auto& bar = g_mixed_bar;
     constexpr int MB = kMb[R];
-    constexpr int N = kNB * Z;
-    constexpr int G = THREADS / Z;
-    constexpr int BUF = 24 * THREADS;          /* floats per buffer set (all slots) */
-    static_assert(G >= 1 && G <= kMixedMaxSlots, "slots per CTA");
-    static_assert(kMixedMaxChunk <= THREADS, "one thread per frame of an item");
+    constexpr int NBLK = num_blocks(R);
+    const MixedCode& code = a.codes[item.variant - R * kNumZ];
+    const int z = code.z, n = code.n;
+    const int G = THREADS / z;
     const int tid = threadIdx.x;
-    const int g = tid / Z;
-    const int r = tid - g * Z;
+    const int g = tid / z;
+    const int r = tid - g * z;
     const bool in_slot = g < G;
-
-    /* issue the bulk copy of the item's j-th frame into buffer b of slot q (thread 0) */
-    auto fetch = [&](int q, int b, int j) {
-        const long long off = S.olist[j];
-        S.pre[q] = S.flist[j];
-        S.off_pre[q] = off;
-        fence_proxy_async_smem();   /* earlier generic reads of that buffer come first */
-        mbar_arrive_expect_tx(&bar[b][q], (uint32_t)(N * 4));
-        bulk_g2s(smem + b * BUF + q * N, a.llr + off, (uint32_t)(N * 4), &bar[b][q]);
-    };
-
-    /* the item's frame list and offsets into shared memory, one per thread */
+    float* const P = smem + (in_slot ? g : 0) * n;
+    unsigned short* const A = reinterpret_cast<unsigned short*>(smem + 24 * THREADS);
+    /* this thread's edge addresses for the item's code, [block][thread] */
+    for (int b = 0; b < NBLK; b++) {
+        int t = r + (int)code.shift[b];
+        t = t >= z ? t - z : t;
+        A[b * THREADS + tid] = in_slot ? (unsigned short)(code.colz[b] + t) : (unsigned short)0;
+    }
+    auto addr = [&](int b) -> int { return A[b * THREADS + tid]; };
+    /* the item's frame list and offsets, one per thread */
     if (tid < item.count) {
         const int f = a.perm[item.start + tid];
         S.flist[tid] = f;
         S.olist[tid] = a.offset[f];
     }
-    __syncthreads();
     if (tid == 0) {
         S.next = 0;
         S.abort = 0;
-        for (int q = 0; q < G; q++) {
-            S.frame[q] = -1;
-            S.pre[q] = -1;
-            const int b = ((S.cur >> q) & 1u) ^ 1u;
-            if (S.next < item.count) fetch(q, b, S.next++);
-        }
+        for (int q = 0; q < G; q++) S.frame[q] = -1;
     }
-    __syncthreads();
 
     /* messages: registers (every index a compile-time constant), or shared
-     * memory after the two buffer sets, [3][kMaxMb][THREADS] */
+     * memory after the address table, [3][kMaxMb][THREADS] */
     float rM1[MB], rM2[MB];
     uint32_t rNEG[MB];
-    float* const sM1 = smem + 2 * BUF + tid;
+    float* const sM1 = smem + 24 * THREADS + 48 * THREADS + tid;
     float* const sM2 = sM1 + kMaxMb * THREADS;
     uint32_t* const sNEG = reinterpret_cast<uint32_t*>(sM2 + kMaxMb * THREADS);
 
     int frame = -1, iters = 0;
     long long off = 0;
     bool need_check = false;
-    float* P = smem;
+    __syncthreads();
 
     while (true) {
-        /* 1. slots that are empty and have a prefetched frame: wait for its copy */
-        const int my_pre = in_slot ? S.pre[g] : -1;
-        if (in_slot && frame < 0 && my_pre >= 0) {
-            const int b = ((S.cur >> g) & 1u) ^ 1u;
-            if (!mbar_wait_bounded(&bar[b][g], (S.phase >> (8 * b + g)) & 1u)) atomicOr(&S.abort, 1u);
-        }
-        __syncthreads();
-        if (S.abort) break;
+        /* 1. refill empty slots: thread 0 hands out the item's next frames and
+         * starts one bulk copy per refilled slot into its posterior buffer */
         if (tid == 0) {
             unsigned fresh = 0;
-            for (int q = 0; q < G; q++) {
-                if (S.frame[q] >= 0 || S.pre[q] < 0) continue;
-                const int b = ((S.cur >> q) & 1u) ^ 1u;
-                S.phase ^= 1u << (8 * b + q);
-                S.cur ^= 1u << q;
-                S.frame[q] = S.pre[q];
-                S.off_cur[q] = S.off_pre[q];
-                S.pre[q] = -1;
-                fresh |= 1u << q;
-                if (S.next < item.count) fetch(q, b ^ 1, S.next++);
-            }
+            for (int q = 0; q < G; q++)
+                if (S.frame[q] < 0 && S.next < item.count) {
+                    const int j = S.next++;
+                    S.frame[q] = S.flist[j];
+                    S.off[q] = S.olist[j];
+                    fresh |= 1u << q;
+                    fence_proxy_async_smem();   /* the slot's earlier generic reads come first */
+                    mbar_arrive_expect_tx(&bar[q], (uint32_t)(n * 4));
+                    bulk_g2s(smem + q * n, a.llr + S.olist[j], (uint32_t)(n * 4), &bar[q]);
+                }
             S.fresh = fresh;
             S.fail = 0;
         }
         __syncthreads();
         if (in_slot && ((S.fresh >> g) & 1u)) {
             frame = S.frame[g];
-            off = S.off_cur[g];
-            P = smem + ((S.cur >> g) & 1u) * BUF + g * N;
+            off = S.off[g];
             iters = 0;
             need_check = true;
+            if (!mbar_wait_bounded(&bar[g], (S.phase >> g) & 1u)) atomicOr(&S.abort, 1u);
             static_for<MB>([&](auto I) {
                 constexpr int i = decltype(I)::value;
                 if constexpr (LAYOUT == kMsgRegisters) {
@@ -182,13 +147,14 @@ __device__ __noinline__ bool mixed_item(const MixedArgs& a, const MixedItem item
                 }
             });
         }
-        float* const Pr = P + r;
-        float* const Prz = Pr - Z;
+        __syncthreads();
+        if (S.abort) break;
+        if (tid == 0) S.phase ^= S.fresh;   /* every refilled slot's barrier completed one phase */
 
         /* 2. syndrome of the slots loaded or iterated since their last check */
         if (in_slot && frame >= 0 && need_check) {
             const unsigned fail = tdmp_rows_fail<R>([&](auto I, auto E) {
-                return edge_ptr<R, Z, decltype(I)::value, decltype(E)::value>(Pr, Prz, r);
+                return P + addr(block_index(R, decltype(I)::value, decltype(E)::value));
             });
             if (fail) atomicOr(&S.fail, 1u << g);
         }
@@ -201,7 +167,7 @@ __device__ __noinline__ bool mixed_item(const MixedArgs& a, const MixedItem item
             if (!failed || iters >= a.max_iter) {
 #pragma unroll
                 for (int s = 0; s < 6; s++) {
-                    const int v = r + s * Z;                  /* float4 group of the frame */
+                    const int v = r + s * z;                  /* float4 group of the frame */
                     const float4 p = reinterpret_cast<const float4*>(P)[v];
                     const uint32_t w = (p.x >= 0.0f ? 1u : 0u) | (p.y >= 0.0f ? 1u << 8 : 0u) |
                                        (p.z >= 0.0f ? 1u << 16 : 0u) | (p.w >= 0.0f ? 1u << 24 : 0u);
@@ -217,22 +183,28 @@ __device__ __noinline__ bool mixed_item(const MixedArgs& a, const MixedItem item
         }
         __syncthreads();
 
-        /* 4. done when every slot is empty and nothing is in flight; an empty
-         * slot with a prefetched frame is refilled before the next iteration */
-        bool all_empty = true, refill = false;
+        /* 4. done when every slot is empty and no frame is left; an empty
+         * slot is refilled before the next iteration while frames remain */
+        bool any_empty = false, all_empty = true;
         for (int q = 0; q < G; q++) {
-            all_empty &= S.frame[q] < 0 && S.pre[q] < 0;
-            refill |= S.frame[q] < 0 && S.pre[q] >= 0;
+            any_empty |= S.frame[q] < 0;
+            all_empty &= S.frame[q] < 0;
         }
-        if (all_empty) break;
-        if (refill) continue;
+        const bool more = S.next < item.count;
+        __syncthreads();
+        if (all_empty && !more) break;
+        if (any_empty && more) continue;
 
         /* 5. one iteration of every occupied slot (all of them failed their check) */
         const bool active = in_slot && frame >= 0;
         static_for<MB>([&](auto I) {
             constexpr int i = decltype(I)::value;
+            constexpr int d = layer_degree(R, i);
             if (active) {
-                auto at = [&](auto E) { return edge_ptr<R, Z, i, decltype(E)::value>(Pr, Prz, r); };
+                /* the layer's edge addresses, loaded once for both passes */
+                int ad[d];
+                static_for<d>([&](auto E) { ad[decltype(E)::value] = addr(block_index(R, i, decltype(E)::value)); });
+                auto at = [&](auto E) { return P + ad[decltype(E)::value]; };
                 if constexpr (LAYOUT == kMsgRegisters) {
                     tdmp_layer<R, i, kNms>(at, rM1[i], rM2[i], rNEG[i]);
                 } else {
@@ -252,32 +224,29 @@ __device__ __noinline__ bool mixed_item(const MixedArgs& a, const MixedItem item
         }
     }
     if (S.abort) {
-        /* a staging wait expired: record it, let every copy in flight land, stop */
+        /* a staging wait expired: record it and let every copy in flight land */
         if (tid == 0) {
             atomicOr(a.err, kErrWaitTimeout);
             for (int q = 0; q < G; q++)
-                if (S.pre[q] >= 0) {
-                    const int b = ((S.cur >> q) & 1u) ^ 1u;
-                    mbar_wait_bounded(&bar[b][q], (S.phase >> (8 * b + q)) & 1u);
-                }
+                if ((S.fresh >> q) & 1u) mbar_wait_bounded(&bar[q], (S.phase >> q) & 1u);
         }
         return false;
     }
     return true;
 }
 
-/* One persistent grid per rate: items of any z of rate R, each decoded by the
- * body specialised on its z. */
+/* One persistent grid per rate: it takes work items of its rate from its own
+ * queue until none are left. */
 template <int R, int THREADS, int LAYOUT>
-__global__ void __launch_bounds__(THREADS, (MixedOcc<THREADS, LAYOUT>::MIN_CTAS))
+__global__ void __launch_bounds__(THREADS, (MixedOcc<THREADS>::MIN_CTAS))
 mixed_decode_kernel(const __grid_constant__ MixedArgs a)
 {
-    MixedCtl& S = g_mixed_ctl;
+    extern __shared__ __align__(128) float smem_mixed[];
+    __shared__ __align__(8) uint64_t bar[kMixedMaxSlots];
+    __shared__ MixedCtl S;
     if (threadIdx.x == 0) {
-        for (int b = 0; b < 2; b++)
-            for (int q = 0; q < kMixedMaxSlots; q++) mbar_init(&g_mixed_bar[b][q], 1);
+        for (int q = 0; q < kMixedMaxSlots; q++) mbar_init(&bar[q], 1);
         fence_mbar_init();
-        S.cur = 0xffffffffu;     /* first frames go into buffer 0 */
         S.phase = 0;
     }
     const MixedItem* items = a.items + (long long)R * a.items_per_rate;
@@ -287,14 +256,7 @@ mixed_decode_kernel(const __grid_constant__ MixedArgs a)
         const int k = S.item;
         __syncthreads();
         if (k >= a.num_items[R]) break;
-        const MixedItem it = items[k];
-        const int zi = it.variant - R * kNumZ;
-        bool ok = true;
-        static_for<kNumZ>([&](auto ZI) {
-            constexpr int zi_c = decltype(ZI)::value;
-            if (zi == zi_c) ok = mixed_item<R, kZMin + kZStep * zi_c, THREADS, LAYOUT>(a, it);
-        });
-        if (!ok) break;
+        if (!mixed_item<R, THREADS, LAYOUT>(a, items[k], smem_mixed, S, bar)) break;
         __syncthreads();
     }
 }
