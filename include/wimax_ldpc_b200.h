@@ -163,6 +163,12 @@ WLDPC_API int wldpc_decoder_synchronize(wldpc_decoder* dec);
  * Outputs of such a launch are undefined. */
 #define WLDPC_WAIT_LIMIT_DEFAULT (1u << 22)
 WLDPC_API int wldpc_decoder_set_wait_limit(wldpc_decoder* dec, unsigned polls);
+/* No counterpart in the reference: measures the time bound of the kernels'
+ * waits. One GPU thread polls, `polls` times (at most 2^24), the mbarrier
+ * phase of a barrier that never completes, as the decoders poll their
+ * staging barrier, and *elapsed_ns receives the device time it took.
+ * Synchronous, on the default stream. */
+WLDPC_API int wldpc_wait_bound_ns(unsigned polls, uint64_t* elapsed_ns);
 
 /* ---------------------------------------------------------------- encoder */
 

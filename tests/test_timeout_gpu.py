@@ -40,3 +40,14 @@ def test_staging_wait_timeout_is_reported_and_the_next_call_is_clean(wl, cuda, o
     assert ((status.cpu().numpy() & 0xFFFF) == io).all()
     post, h2, ne, st = dec.decode_host(llr)
     assert (post.view(np.uint32) == po.view(np.uint32)).all() and (h2 == do).all()
+
+
+def test_wait_bound_is_under_a_second(wl, cuda):
+    """The decoders' waits give up after WLDPC_WAIT_LIMIT_DEFAULT polls; on a
+    barrier that never completes those polls must end well within a second
+    (the documented bound), and scale with the poll count."""
+    small = wl.wait_bound_ns(1 << 16)
+    full = wl.wait_bound_ns(wl.WAIT_LIMIT_DEFAULT)
+    print(f"wait bound: {small / 1e6:.3f} ms for 2^16 polls, {full / 1e6:.3f} ms for 2^22")
+    assert 0 < small < full
+    assert full < 1e9

@@ -78,6 +78,7 @@ def _lib():
     L.wldpc_decode_batch_host.argtypes = [_p, _p, _p, _p, _p, _sz]
     L.wldpc_decode_batch_host_hard.argtypes = [_p, _p, _p, _p, _p, _sz]
     L.wldpc_decoder_set_wait_limit.argtypes = [_p, _u]
+    L.wldpc_wait_bound_ns.argtypes = [_u, ctypes.POINTER(ctypes.c_uint64)]
     L.wldpc_decode_bits_batch_host.argtypes = [_p, _p, _p, _p, _sz]
     L.wldpc_syndrome_batch_host.argtypes = [_p, _p, _i, _p, _sz]
     L.wldpc_encode_batch_host.argtypes = [_p, _p, _p, _sz]
@@ -152,6 +153,14 @@ def _stream_ptr(stream):
         import torch
         stream = torch.cuda.current_stream()
     return ctypes.c_void_p(stream.cuda_stream)
+
+
+def wait_bound_ns(polls: int = WAIT_LIMIT_DEFAULT) -> int:
+    """Device nanoseconds that `polls` polls of a never-completing barrier take
+    (the time bound of the kernels' staging waits at that limit)."""
+    ns = ctypes.c_uint64()
+    _check(_lib().wldpc_wait_bound_ns(polls, ctypes.byref(ns)), "wait_bound_ns")
+    return ns.value
 
 
 def code_info(rate: int, z: int) -> CodeInfo:

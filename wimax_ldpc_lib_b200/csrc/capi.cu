@@ -262,6 +262,21 @@ int wldpc_decoder_set_wait_limit(wldpc_decoder* d, unsigned polls)
     return WLDPC_OK;
 }
 
+int wldpc_wait_bound_ns(unsigned polls, uint64_t* elapsed_ns)
+{
+    if (!elapsed_ns || polls > (1u << 24)) return WLDPC_ERR_ARG;
+    int rc = check_device();
+    if (rc) return rc;
+    DevBuf out;
+    if ((rc = out.reserve(2 * sizeof(unsigned long long)))) return rc;
+    unsigned long long h[2] = {0, 0};
+    CU(launch_wait_bound(polls, (unsigned long long*)out.p, 0));
+    CU(cudaMemcpy(h, out.p, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h[1]) return WLDPC_ERR_CUDA;   /* a barrier nobody completes cannot have completed */
+    *elapsed_ns = h[0];
+    return WLDPC_OK;
+}
+
 int wldpc_decoder_synchronize(wldpc_decoder* d)
 {
     if (!d) return WLDPC_ERR_ARG;
