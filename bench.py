@@ -28,6 +28,8 @@ and is no worse than the plain decoder's, else the plain one's.
   config2    131072 frames mixed over all 114 codes, one graph launch
   encoder    the dual-diagonal encoder on the headline batch
   single_frame  decode(float*) one frame per call, next to one reference core
+  waterfall  rate 1/2 z=96 BER/FER sweep (0.1 dB steps, >= 200 bit errors per
+             point) with the plain and the fp32 learned decoder: Eb/N0 at BER 1e-5
 
 Multi-GPU: every rank decodes its own shard of frames (weak scaling, no
 data-path collective); timing is the max over ranks, counters are summed.
@@ -63,7 +65,7 @@ C1_K = 20 * C1_Z
 # config 2: mixed batch over all 114 codes
 MIXED_FRAMES = 131072
 WEIGHTS_DIR = os.path.join(ROOT, "wimax_ldpc_lib_b200", "weights")
-SECTIONS = ("e2e", "config1", "config2", "encoder", "single_frame")
+SECTIONS = ("e2e", "config1", "config2", "encoder", "single_frame", "waterfall")
 
 
 def load_peaks():
@@ -585,6 +587,26 @@ def run_ours(args):
             sf["reference_one_core"] = {"frames_per_s": src1.shape[0] / dt, "latency_us": 1e6 * dt / src1.shape[0],
                                         "info_gbps": src1.shape[0] * k / dt / 1e9}
         extra["single_frame"] = sf
+
+    # config 4 for the headline code: the full-device waterfall of the plain and
+    # the fp32 learned decoder (generation, encoding, channel, decoding and
+    # counting on the device), rank 0 only (no collective inside)
+    if "waterfall" in sections and rank == 0:
+        from wimax_ldpc_lib_b200 import waterfall as wf
+        t0 = time.perf_counter()
+        wres = {}
+        for name in ("plain", "learned"):
+            if name not in decoders:
+                continue
+            pts = wf.sweep(RATE, Z, decoders[name], start=1.6, step=0.1, min_errors=200, max_bits=4e8,
+                           stop_ber=1e-6, batch=1 << 17, max_points=12, log=lambda *a: None)
+            wres[name] = {"ebno_at_ber_1e-5": wf.ebno_at(pts), "points": len(pts),
+                          "frames": sum(p["frames"] for p in pts),
+                          "ber": {f"{p['ebno_db']:.1f}": p["ber"] for p in pts},
+                          "fer": {f"{p['ebno_db']:.1f}": p["fer"] for p in pts}}
+        extra["waterfall"] = {"workload": "rate 1/2 z=96, Eb/N0 from 1.6 dB in 0.1 dB steps until BER < 1e-6, >= 200 "
+                                          "info-bit errors (or 4e8 bits) per point, cap 10, all on the device",
+                              "decoders": wres, "seconds": time.perf_counter() - t0}
 
     if rank == 0:
         T = lms_meta["iterations"] if lms_meta else 8

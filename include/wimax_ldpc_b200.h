@@ -155,20 +155,20 @@ WLDPC_API int wldpc_syndrome_batch_host(wldpc_decoder* dec, const int8_t* bits, 
 WLDPC_API int wldpc_decoder_synchronize(wldpc_decoder* dec);
 
 /* No counterpart in the reference (it has no device waits): a test hook that
- * sets how many times the decode kernel polls the barrier of its frame
- * staging copy before giving up (default WLDPC_WAIT_LIMIT_DEFAULT, well under
- * a second). With 0 every launch gives up at once: it records a timeout,
- * waits (with the default bound) for its copy to land and exits, and the
- * next synchronising call returns WLDPC_ERR_TIMEOUT with the context intact.
- * Outputs of such a launch are undefined. */
-#define WLDPC_WAIT_LIMIT_DEFAULT (1u << 22)
-WLDPC_API int wldpc_decoder_set_wait_limit(wldpc_decoder* dec, unsigned polls);
-/* No counterpart in the reference: measures the time bound of the kernels'
- * waits. One GPU thread polls, `polls` times (at most 2^24), the mbarrier
- * phase of a barrier that never completes, as the decoders poll their
- * staging barrier, and *elapsed_ns receives the device time it took.
- * Synchronous, on the default stream. */
-WLDPC_API int wldpc_wait_bound_ns(unsigned polls, uint64_t* elapsed_ns);
+ * sets how long (device time, microseconds) the decode kernel waits for the
+ * barrier of its frame staging copy before giving up (default
+ * WLDPC_WAIT_LIMIT_DEFAULT_US, one second). With 0 every launch gives up at
+ * once: it records a timeout, waits (with the default bound) for its copy
+ * to land and exits, and the next synchronising call returns
+ * WLDPC_ERR_TIMEOUT with the context intact. Outputs of such a launch are
+ * undefined. */
+#define WLDPC_WAIT_LIMIT_DEFAULT_US 1000000u
+WLDPC_API int wldpc_decoder_set_wait_limit(wldpc_decoder* dec, unsigned limit_us);
+/* No counterpart in the reference: measures the kernels' wait bound. One GPU
+ * thread runs the bounded wait with limit limit_us (at most ten times the
+ * default) on an mbarrier phase that never completes, and *elapsed_ns
+ * receives the device time until it gave up. Synchronous, default stream. */
+WLDPC_API int wldpc_wait_bound_ns(unsigned limit_us, uint64_t* elapsed_ns);
 
 /* ---------------------------------------------------------------- encoder */
 

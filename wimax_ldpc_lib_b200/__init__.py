@@ -28,7 +28,7 @@ MIXED_CONCURRENT, MIXED_SERIAL = 0, 1           # mixed decoder launch policy of
 
 OK = 0
 ERR_ARG, ERR_CODE, ERR_CUDA, ERR_NO_DEVICE, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_SCRATCH = -1, -2, -3, -4, -5, -6, -7
-WAIT_LIMIT_DEFAULT = 1 << 22   # WLDPC_WAIT_LIMIT_DEFAULT
+WAIT_LIMIT_DEFAULT_US = 1000000   # WLDPC_WAIT_LIMIT_DEFAULT_US: bound of the kernels' waits
 
 _p = ctypes.c_void_p
 _i = ctypes.c_int
@@ -155,11 +155,11 @@ def _stream_ptr(stream):
     return ctypes.c_void_p(stream.cuda_stream)
 
 
-def wait_bound_ns(polls: int = WAIT_LIMIT_DEFAULT) -> int:
-    """Device nanoseconds that `polls` polls of a never-completing barrier take
-    (the time bound of the kernels' staging waits at that limit)."""
+def wait_bound_ns(limit_us: int = WAIT_LIMIT_DEFAULT_US) -> int:
+    """Device nanoseconds the kernels' bounded wait with that limit takes on a
+    barrier that never completes."""
     ns = ctypes.c_uint64()
-    _check(_lib().wldpc_wait_bound_ns(polls, ctypes.byref(ns)), "wait_bound_ns")
+    _check(_lib().wldpc_wait_bound_ns(limit_us, ctypes.byref(ns)), "wait_bound_ns")
     return ns.value
 
 
@@ -276,9 +276,9 @@ class Decoder:
         _check(_lib().wldpc_decode_batch_device(self._h, _t_ptr(llr), _t_ptr(decoded), _t_ptr(posterior),
                                                 _t_ptr(status), frames, _stream_ptr(stream)), "decode_batch_device")
 
-    def set_wait_limit(self, polls: int) -> None:
-        """Test hook: polls of the kernel's staging wait (0 = time out at once)."""
-        _check(_lib().wldpc_decoder_set_wait_limit(self._h, polls), "set_wait_limit")
+    def set_wait_limit(self, limit_us: int) -> None:
+        """Test hook: bound of the kernel's staging wait in microseconds (0 = time out at once)."""
+        _check(_lib().wldpc_decoder_set_wait_limit(self._h, limit_us), "set_wait_limit")
 
     def synchronize(self):
         _check(_lib().wldpc_decoder_synchronize(self._h), "synchronize")

@@ -85,7 +85,7 @@ static int drain_pipe(cudaStream_t (&pipe)[S], int rc)
 struct wldpc_decoder {
     int rate, z, mode;
     unsigned max_iter;
-    unsigned wait_limit = kWaitLimit;   /* polls of the kernel's staging wait (test hook) */
+    unsigned wait_limit_us = kWaitLimitUs;   /* bound of the kernel's staging wait (test hook) */
     CodeDesc code;
     cudaStream_t stream = nullptr;
     cudaStream_t pipe[kHostStages] = {};
@@ -228,7 +228,7 @@ static int decode_launch(wldpc_decoder* d, const float* llr, int8_t* hard, float
     a.err = d->err;
     a.frames = (long long)frames;
     a.max_iter = (int)d->max_iter;
-    a.wait_limit = d->wait_limit;
+    a.wait_limit_us = d->wait_limit_us;
     return launch_tdmp(d->rate, d->z, d->mode, a, st) == cudaSuccess ? WLDPC_OK : WLDPC_ERR_CUDA;
 }
 
@@ -253,24 +253,24 @@ int wldpc_decode_batch_device(wldpc_decoder* d, const float* llr, int8_t* decode
     return decode_launch(d, llr, decoded, posterior, status, frames, (cudaStream_t)stream);
 }
 
-static_assert(kWaitLimit == WLDPC_WAIT_LIMIT_DEFAULT, "the header's default wait limit is the kernels'");
+static_assert(kWaitLimitUs == WLDPC_WAIT_LIMIT_DEFAULT_US, "the header's default wait limit is the kernels'");
 
-int wldpc_decoder_set_wait_limit(wldpc_decoder* d, unsigned polls)
+int wldpc_decoder_set_wait_limit(wldpc_decoder* d, unsigned limit_us)
 {
     if (!d) return WLDPC_ERR_ARG;
-    d->wait_limit = polls;
+    d->wait_limit_us = limit_us;
     return WLDPC_OK;
 }
 
-int wldpc_wait_bound_ns(unsigned polls, uint64_t* elapsed_ns)
+int wldpc_wait_bound_ns(unsigned limit_us, uint64_t* elapsed_ns)
 {
-    if (!elapsed_ns || polls > (1u << 24)) return WLDPC_ERR_ARG;
+    if (!elapsed_ns || limit_us > 10u * kWaitLimitUs) return WLDPC_ERR_ARG;
     int rc = check_device();
     if (rc) return rc;
     DevBuf out;
     if ((rc = out.reserve(2 * sizeof(unsigned long long)))) return rc;
     unsigned long long h[2] = {0, 0};
-    CU(launch_wait_bound(polls, (unsigned long long*)out.p, 0));
+    CU(launch_wait_bound(limit_us, (unsigned long long*)out.p, 0));
     CU(cudaMemcpy(h, out.p, sizeof(h), cudaMemcpyDeviceToHost));
     if (h[1]) return WLDPC_ERR_CUDA;   /* a barrier nobody completes cannot have completed */
     *elapsed_ns = h[0];

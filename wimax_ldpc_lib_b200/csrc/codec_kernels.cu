@@ -279,28 +279,26 @@ __global__ void lfsr_bits_kernel(unsigned long long first_bit, long long nbits, 
     }
 }
 
-/* How long `polls` polls of an mbarrier phase that never completes take: one
- * thread initialises a barrier expecting two arrivals, arrives once, runs
- * the decoders' bounded wait on it and records the elapsed global-timer
- * nanoseconds and whether the wait (wrongly) succeeded. Nothing is copied,
- * so nothing is in flight when the thread exits. */
-__global__ void wait_bound_kernel(uint32_t polls, unsigned long long* out)
+/* How long the decoders' bounded wait with limit limit_us takes on an
+ * mbarrier phase that never completes: one thread initialises a barrier
+ * expecting two arrivals, arrives once, runs the wait on it and records the
+ * elapsed global-timer nanoseconds and whether the wait (wrongly)
+ * succeeded. Nothing is copied, so nothing is in flight when it exits. */
+__global__ void wait_bound_kernel(uint32_t limit_us, unsigned long long* out)
 {
     __shared__ __align__(8) uint64_t bar;
     mbar_init(&bar, 2);
     fence_mbar_init();
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&bar)) : "memory");
-    unsigned long long t0, t1;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-    const bool ok = mbar_wait_bounded(&bar, 0, polls);
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-    out[0] = t1 - t0;
+    const unsigned long long t0 = global_ns();
+    const bool ok = mbar_wait_bounded(&bar, 0, limit_us);
+    out[0] = global_ns() - t0;
     out[1] = ok ? 1ull : 0ull;
 }
 
-cudaError_t launch_wait_bound(uint32_t polls, unsigned long long* out, cudaStream_t st)
+cudaError_t launch_wait_bound(uint32_t limit_us, unsigned long long* out, cudaStream_t st)
 {
-    wait_bound_kernel<<<1, 1, 0, st>>>(polls, out);
+    wait_bound_kernel<<<1, 1, 0, st>>>(limit_us, out);
     return cudaGetLastError();
 }
 

@@ -43,7 +43,7 @@ cudaError_t launch_syndrome(const CodeDesc& c, const int8_t* bits, uint32_t* out
 cudaError_t launch_bits_to_llr(const int8_t* bits, float* llr, long long count, cudaStream_t st);
 /* the reference BER_runner's periodic LFSR info-bit stream */
 cudaError_t upload_lfsr_period(const uint32_t* words);
-cudaError_t launch_wait_bound(uint32_t polls, unsigned long long* out, cudaStream_t st);
+cudaError_t launch_wait_bound(uint32_t limit_us, unsigned long long* out, cudaStream_t st);
 cudaError_t launch_lfsr_bits(unsigned long long first_bit, long long nbits, uint8_t* out, cudaStream_t st);
 
 /* TDMP decoder specialised on (rate, z, mode) */

@@ -130,16 +130,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase)
     return ok != 0;
 }
 
-/* Bounded wait on an mbarrier phase. Each try_wait blocks for a hardware
- * time slice, so kWaitLimit tries bound the wait to well under a second on a
- * healthy GPU; on expiry the caller records kErrWaitTimeout and bails out.
- * limit = 0 gives up at once (the decoders' wait-limit test hook uses it). */
-constexpr uint32_t kWaitLimit = 1u << 22;
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t limit = kWaitLimit)
+__device__ __forceinline__ uint64_t global_ns()
 {
-    for (uint32_t i = 0; i < limit; ++i)
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+/* Bounded wait on an mbarrier phase: polls until the phase completes or
+ * limit_us microseconds of device time (%globaltimer) have passed. A bound
+ * by poll count is not a time bound: one try_wait suspends the thread for an
+ * implementation-defined slice, measured at about 4 us on B200, so 2^22
+ * polls took 16.6 s. On expiry the caller records kErrWaitTimeout and bails
+ * out. limit_us = 0 gives up at once (the decoders' wait-limit test hook). */
+constexpr uint32_t kWaitLimitUs = 1000000u;   /* one second */
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t limit_us = kWaitLimitUs)
+{
+    if (limit_us == 0) return false;
+    const uint64_t t0 = global_ns();
+    const uint64_t limit_ns = (uint64_t)limit_us * 1000u;
+    while (true) {
         if (mbar_try_wait(bar, phase)) return true;
-    return false;
+        if (global_ns() - t0 >= limit_ns) return false;
+    }
 }
 
 __host__ __device__ constexpr int gcd_c(int a, int b) { return b == 0 ? a : gcd_c(b, a % b); }

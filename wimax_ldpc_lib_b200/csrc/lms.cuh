@@ -71,7 +71,7 @@ struct LmsArgs {
     long long frames;
     int iters;              /* iteration cap */
     int wrows;              /* trained iterations T <= kLmsMaxIter; iteration t >= T uses row T-1 */
-    unsigned wait_limit = kWaitLimit;   /* polls of the staging wait (the drain wait after a timeout is full) */
+    unsigned wait_limit_us = kWaitLimitUs;   /* bound of the staging wait (the drain wait after a timeout is full) */
     float2 wab[kLmsMaxIter][kLmsMaxBlocks];   /* (a, b) per (iteration, block): one 8-byte load per edge */
 };
 
@@ -127,11 +127,11 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         bulk_g2s(smem_lms, a.llr + f0 * N, bytes, &bar);
     }
     __syncthreads();
-    const bool ok = mbar_wait_bounded(&bar, 0, a.wait_limit);
+    const bool ok = mbar_wait_bounded(&bar, 0, a.wait_limit_us);
     if (__syncthreads_or(!ok)) {
         if (tid == 0) {
             atomicOr(a.err, kErrWaitTimeout);
-            mbar_wait_bounded(&bar, 0, kWaitLimit);   /* let an in-flight copy land before exit */
+            mbar_wait_bounded(&bar, 0, kWaitLimitUs);   /* let an in-flight copy land before exit */
         }
         return;
     }

@@ -57,7 +57,7 @@ struct DecodeArgs {
     unsigned* err;          /* error word (kErr*) */
     long long frames;
     int max_iter;
-    unsigned wait_limit = kWaitLimit;   /* polls of the staging wait (the drain wait after a timeout is full) */
+    unsigned wait_limit_us = kWaitLimitUs;   /* bound of the staging wait (the drain wait after a timeout is full) */
     /* used only by the kernels whose z is a run-time value (ZT == 0): */
     int z;
     unsigned short shift[96];   /* per non-zero block, row-major over base rows */
@@ -270,11 +270,11 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
         bulk_g2s(smem_post, a.llr + f0 * N, bytes, &bar);
     }
     __syncthreads();
-    const bool ok = mbar_wait_bounded(&bar, 0, a.wait_limit);
+    const bool ok = mbar_wait_bounded(&bar, 0, a.wait_limit_us);
     if (__syncthreads_or(!ok)) {
         if (tid == 0) {
             atomicOr(a.err, kErrWaitTimeout);
-            mbar_wait_bounded(&bar, 0, kWaitLimit);   /* let an in-flight copy land before exit */
+            mbar_wait_bounded(&bar, 0, kWaitLimitUs);   /* let an in-flight copy land before exit */
         }
         return;
     }
