@@ -93,6 +93,7 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
     if (tid == 0) {
         S.next = 0;
         S.abort = 0;
+        S.fail = 0;
         for (int q = 0; q < G; q++) S.frame[q] = -1;
     }
 
@@ -107,49 +108,53 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
     int frame = -1, iters = 0;
     long long off = 0;
     bool need_check = false;
+    bool refill = true;   /* uniform: some slot is empty and the item has frames left */
     __syncthreads();
 
     while (true) {
-        /* 1. refill empty slots: thread 0 hands out the item's next frames and
-         * starts one bulk copy per refilled slot into its posterior buffer */
-        if (tid == 0) {
-            unsigned fresh = 0;
-            for (int q = 0; q < G; q++)
-                if (S.frame[q] < 0 && S.next < item.count) {
-                    const int j = S.next++;
-                    S.frame[q] = S.flist[j];
-                    S.off[q] = S.olist[j];
-                    fresh |= 1u << q;
-                    fence_proxy_async_smem();   /* the slot's earlier generic reads come first */
-                    mbar_arrive_expect_tx(&bar[q], (uint32_t)(n * 4));
-                    bulk_g2s(smem + q * n, a.llr + S.olist[j], (uint32_t)(n * 4), &bar[q]);
-                }
-            S.fresh = fresh;
-            S.fail = 0;
+        /* 1. refill empty slots (only when one is empty, so an iteration without
+         * a converged frame costs no barrier here): thread 0 hands out the
+         * item's next frames and starts one bulk copy per refilled slot into
+         * its posterior buffer */
+        if (refill) {
+            if (tid == 0) {
+                unsigned fresh = 0;
+                for (int q = 0; q < G; q++)
+                    if (S.frame[q] < 0 && S.next < item.count) {
+                        const int j = S.next++;
+                        S.frame[q] = S.flist[j];
+                        S.off[q] = S.olist[j];
+                        fresh |= 1u << q;
+                        fence_proxy_async_smem();   /* the slot's earlier generic reads come first */
+                        mbar_arrive_expect_tx(&bar[q], (uint32_t)(n * 4));
+                        bulk_g2s(smem + q * n, a.llr + S.olist[j], (uint32_t)(n * 4), &bar[q]);
+                    }
+                S.fresh = fresh;
+            }
+            __syncthreads();
+            if (in_slot && ((S.fresh >> g) & 1u)) {
+                frame = S.frame[g];
+                off = S.off[g];
+                iters = 0;
+                need_check = true;
+                if (!mbar_wait_bounded(&bar[g], (S.phase >> g) & 1u)) atomicOr(&S.abort, 1u);
+                static_for<MB>([&](auto I) {
+                    constexpr int i = decltype(I)::value;
+                    if constexpr (LAYOUT == kMsgRegisters) {
+                        rM1[i] = 0.0f;
+                        rM2[i] = 0.0f;
+                        rNEG[i] = 0u;
+                    } else {
+                        sM1[i * THREADS] = 0.0f;
+                        sM2[i * THREADS] = 0.0f;
+                        sNEG[i * THREADS] = 0u;
+                    }
+                });
+            }
+            __syncthreads();
+            if (S.abort) break;
+            if (tid == 0) S.phase ^= S.fresh;   /* every refilled slot's barrier completed one phase */
         }
-        __syncthreads();
-        if (in_slot && ((S.fresh >> g) & 1u)) {
-            frame = S.frame[g];
-            off = S.off[g];
-            iters = 0;
-            need_check = true;
-            if (!mbar_wait_bounded(&bar[g], (S.phase >> g) & 1u)) atomicOr(&S.abort, 1u);
-            static_for<MB>([&](auto I) {
-                constexpr int i = decltype(I)::value;
-                if constexpr (LAYOUT == kMsgRegisters) {
-                    rM1[i] = 0.0f;
-                    rM2[i] = 0.0f;
-                    rNEG[i] = 0u;
-                } else {
-                    sM1[i * THREADS] = 0.0f;
-                    sM2[i * THREADS] = 0.0f;
-                    sNEG[i * THREADS] = 0u;
-                }
-            });
-        }
-        __syncthreads();
-        if (S.abort) break;
-        if (tid == 0) S.phase ^= S.fresh;   /* every refilled slot's barrier completed one phase */
 
         /* 2. syndrome of the slots loaded or iterated since their last check */
         if (in_slot && frame >= 0 && need_check) {
@@ -191,9 +196,13 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
             all_empty &= S.frame[q] < 0;
         }
         const bool more = S.next < item.count;
-        __syncthreads();
+        if (tid == 0) S.fail = 0;   /* read only in step 3, before the barrier above */
         if (all_empty && !more) break;
-        if (any_empty && more) continue;
+        refill = any_empty && more;
+        if (refill) {
+            __syncthreads();        /* these reads come before thread 0's refill writes */
+            continue;
+        }
 
         /* 5. one iteration of every occupied slot (all of them failed their check) */
         const bool active = in_slot && frame >= 0;
