@@ -16,10 +16,11 @@
  *
  * Data. The frame's LLRs are staged global -> shared with one TMA bulk copy
  * and updated in place as the posterior (24z floats). Check-to-variable
- * messages live in registers in compressed form per row: the two rounded
- * message magnitudes float(D1), float(D2), the argmin edge and one sign bit per
- * edge. Circulant shifts are compile-time constants: the address of edge e of
- * row r is col*z + (r + shift) mod z.
+ * messages live in registers, either in compressed form per row (the two
+ * rounded message magnitudes float(D1), float(D2), the argmin edge and one
+ * sign bit per edge) or, for the codes where it measured faster, as one
+ * float per edge (tdmp_edge_messages). Circulant shifts are compile-time
+ * constants: the address of edge e of row r is col*z + (r + shift) mod z.
  *
  * Arithmetic that must round exactly as the reference (x86, no FMA):
  *   L = post - msg                      float subtract
@@ -221,6 +222,59 @@ __device__ __forceinline__ void tdmp_layer(At&& at, float& M1, float& M2, uint32
     NEG = ((sgn ^ (flip ? dmask : 0u)) & dmask) | ((uint32_t)nIdx << 27);
 }
 
+/* The same layer with one message per edge kept as a float in a register
+ * (Mr, indexed by block), normalized min-sum only: pass 1 reads the old
+ * message directly instead of rebuilding it from M1 / M2 / NEG. The stored
+ * values are identical to the compressed form's (+-float(D1) or
+ * +-float(D2)): where several edges tie at the minimum, D1 == D2. */
+template <int R, int I, typename At, int NB>
+__device__ __forceinline__ void tdmp_layer_edges(At&& at, float (&Mr)[NB])
+{
+    constexpr int d = layer_degree(R, I);
+    constexpr int b0 = block_index(R, I, 0);
+    float L[d];
+    uint32_t LC[d];
+    uint32_t sgn = 0;
+    float m1, m2;
+    static_for<d>([&](auto E) {
+        constexpr int e = decltype(E)::value;
+        const float l = __fsub_rn(*at(E), Mr[b0 + e]);
+        L[e] = l;
+        LC[e] = __float_as_uint(canon(l));
+        sgn = __funnelshift_l(LC[e], sgn, 1);
+    });
+    two_min_abs<0, d>(L, m1, m2);
+    m1 = fminf(m1, 10000.0f);
+    m2 = fminf(m2, 10000.0f);
+    const uint32_t flip = (uint32_t)((d & 1) ^ (__popc(sgn) & 1));
+    const double D1 = __dmul_rn((double)m1, 0.815), D2 = __dmul_rn((double)m2, 0.815);
+    const float f1 = __double2float_rn(D1), f2 = __double2float_rn(D2);
+    const uint32_t fb = flip << 31;
+    const int h1 = __double2hiint(D1) ^ (int)fb, l1 = __double2loint(D1);
+    const int h2 = __double2hiint(D2) ^ (int)fb, l2 = __double2loint(D2);
+    static_for<d>([&](auto E) {
+        constexpr int e = decltype(E)::value;
+        const float l = L[e];
+        const bool is_min = fabsf(l) == m1;
+        const uint32_t sb = LC[e] & 0x80000000u;
+        int hi = is_min ? h2 : h1;
+        const int lo = is_min ? l2 : l1;
+        hi ^= (int)sb;
+        *at(E) = __double2float_rn(__dadd_rn((double)l, __hiloint2double(hi, lo)));
+        Mr[b0 + e] = __uint_as_float(__float_as_uint(is_min ? f2 : f1) | (sb ^ fb));
+    });
+}
+
+/* Which message layout the specialised normalized min-sum decoder uses: one
+ * float per edge in registers where that measured faster (rate 1/2 at z = 48
+ * and 96: +4% and +7%; rate 2/3B at z = 96: +3%; it needs 128-158 registers,
+ * fewer resident CTAs, and lost 1-9% at the other rates and at z = 24),
+ * else the compressed per-row form (3 registers per layer). */
+constexpr bool tdmp_edge_messages(int rate, int z, int mode)
+{
+    return mode == kNms && ((rate == 0 && (z == 48 || z == 96)) || (rate == 2 && z == 96));
+}
+
 /* Syndrome of the thread's rows over all layers: 1 if any row fails. The
  * hard decision is x >= 0 (-0.0 is bit 1); a row of degree d fails when d
  * minus its number of negative posteriors is odd. at(I, E) as in tdmp_layer. */
@@ -306,21 +360,28 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
     int iters = 0;
 
     /* compressed messages per layer: magnitudes and NEG = sign bits (bit
-     * d-1-e for edge e) | argmin edge << 27 */
+     * d-1-e for edge e) | argmin edge << 27; or one float per edge */
+    constexpr bool EDGE_MSGS = tdmp_edge_messages(R, ZT, MODE);
     float M1[MB], M2[MB];
     uint32_t NEG[MB];
+    float Mr[EDGE_MSGS ? num_blocks(R) : 1];
 #pragma unroll
     for (int i = 0; i < MB; i++) { M1[i] = 0.0f; M2[i] = 0.0f; NEG[i] = 0u; }
+#pragma unroll
+    for (int q = 0; q < (EDGE_MSGS ? num_blocks(R) : 1); q++) Mr[q] = 0.0f;
 
     for (int it = 1; it <= a.max_iter && any_fail; ++it) {
         if constexpr (G > 1) {
             if (tid == 0) s_fail[it & 1] = 0;   /* slot it&1 was last read before the previous barrier */
         }
         static_for<MB>([&](auto I) {
-            if (active)
-                tdmp_layer<R, decltype(I)::value, MODE>(
-                    [&](auto E) { return post_ptr<R, ZT, decltype(I)::value, decltype(E)::value>(P, Pr, Prz, r, a); },
-                    M1[I], M2[I], NEG[I]);
+            if (active) {
+                auto at = [&](auto E) { return post_ptr<R, ZT, decltype(I)::value, decltype(E)::value>(P, Pr, Prz, r, a); };
+                if constexpr (EDGE_MSGS)
+                    tdmp_layer_edges<R, decltype(I)::value>(at, Mr);
+                else
+                    tdmp_layer<R, decltype(I)::value, MODE>(at, M1[I], M2[I], NEG[I]);
+            }
             __syncthreads();
         });
         const bool f = frame_fail(live && active ? rows_fail() : 0u, it & 1, any_fail);
