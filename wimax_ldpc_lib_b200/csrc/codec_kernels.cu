@@ -96,20 +96,32 @@ encode_bytes_kernel(CodeDesc c, const uint8_t* __restrict__ info, uint8_t* __res
     EncScratch& s = scratch[warp];
     const uint8_t* u = info + f * c.k;
     uint8_t* x = cw + f * c.n;
-    /* pack: any non-zero byte is a 1 (reference :43) */
-    const int kw = (c.k + 31) / 32;
-    for (int q = 0; q < kw; q++) {
-        const int j = q * 32 + lane;
-        const uint32_t w = __ballot_sync(0xffffffffu, j < c.k && u[j] != 0);
-        if (lane == 0) s.U[q] = w;
+    /* one pass over the info bytes, 4 per lane (k is a multiple of 4): the
+     * systematic copy of the raw bytes (reference :90) and the packed bits,
+     * any non-zero byte a 1 (reference :43). A lane's 4 bytes give 4 bits;
+     * 8 lanes OR their nibbles into one 32-bit word. */
+    const int kw = (c.k + 31) / 32, k4 = c.k >> 2;
+    const uint32_t* u4 = reinterpret_cast<const uint32_t*>(u);
+    uint32_t* x4 = reinterpret_cast<uint32_t*>(x);
+    for (int base = 0; base < k4; base += 32) {
+        const int j = base + lane;
+        uint32_t v = 0;
+        if (j < k4) {
+            v = u4[j];
+            x4[j] = v;
+        }
+        /* bit t of the nibble: byte t of v is non-zero */
+        const uint32_t nib = (((__vcmpne4(v, 0u) & 0x01010101u) * 0x01020408u) >> 24) & 0xFu;
+        uint32_t wv = nib << (4 * (lane & 7));
+        wv |= __shfl_xor_sync(0xffffffffu, wv, 1);
+        wv |= __shfl_xor_sync(0xffffffffu, wv, 2);
+        wv |= __shfl_xor_sync(0xffffffffu, wv, 4);
+        if ((lane & 7) == 0) s.U[(base >> 3) + (lane >> 3)] = wv;
     }
+    __syncwarp();
     if (lane < 4) s.U[kw + lane] = 0;
     __syncwarp();
     warp_encode_parity(c, s, lane);
-    /* systematic copy of the raw bytes (k is a multiple of 4) */
-    const uint32_t* u4 = reinterpret_cast<const uint32_t*>(u);
-    uint32_t* x4 = reinterpret_cast<uint32_t*>(x);
-    for (int j = lane; j < c.k / 4; j += 32) x4[j] = u4[j];
     /* parity bytes */
     for (int b = 0; b < c.mb; b++)
         for (int r = lane * 4; r < c.z; r += 128)

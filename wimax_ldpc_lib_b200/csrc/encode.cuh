@@ -91,6 +91,13 @@ struct EncScratch {
     uint32_t out[kMaxMb * 3];           /* parity bits to emit, [block][word] */
 };
 
+/* p / nw for the words per block nw in {1, 2, 3} and 0 <= p < 2^15, without
+ * an integer division (p / 3 as a multiply and shift) */
+__device__ __forceinline__ int div_nw(int p, int nw)
+{
+    return nw == 1 ? p : (nw == 2 ? (p >> 1) : (int)(((unsigned)p * 0xAAABu) >> 17));
+}
+
 /* Encodes the packed info bits in s.U into parity words s.out (all lanes of
  * the warp participate; U must be written and visible before the call). */
 __device__ __forceinline__ void warp_encode_parity(const CodeDesc& c, EncScratch& s, int lane)
@@ -98,7 +105,7 @@ __device__ __forceinline__ void warp_encode_parity(const CodeDesc& c, EncScratch
     const int nw = c.nw, z = c.z;
     /* V = H_info * u, one (layer, word) pair per lane */
     for (int p = lane; p < c.mb * nw; p += 32) {
-        const int i = p / nw, w = p - i * nw;
+        const int i = div_nw(p, nw), w = p - i * nw;
         uint32_t v = 0;
         for (int b = c.row_start[i]; b < c.row_start[i + 1]; b++) {
             const int col = c.col[b];
@@ -132,7 +139,7 @@ __device__ __forceinline__ void warp_encode_parity(const CodeDesc& c, EncScratch
     /* F correction: block b >= 1 row r gets P_0[(r + D) mod z]; P_0's words
      * are contiguous at the start of s.P, so it is its own packed column. */
     for (int p = lane; p < c.mb * nw; p += 32) {
-        const int b = p / nw, w = p - b * nw;
+        const int b = div_nw(p, nw), w = p - b * nw;
         uint32_t v = s.P[p];
         if (b > 0) {
             int t = 32 * w + c.D;
