@@ -122,10 +122,13 @@ encode_bytes_kernel(CodeDesc c, const uint8_t* __restrict__ info, uint8_t* __res
     if (lane < 4) s.U[kw + lane] = 0;
     __syncwarp();
     warp_encode_parity(c, s, lane);
-    /* parity bytes */
-    for (int b = 0; b < c.mb; b++)
-        for (int r = lane * 4; r < c.z; r += 128)
-            x4[(c.k + b * c.z + r) / 4] = parity_bytes4(s, c.nw, b, r);
+    /* parity bytes, 4 per lane and store (z is a multiple of 4, so the 4 bits
+     * never straddle a block or a word) */
+    for (int q = lane; q < c.m >> 2; q += 32) {
+        const int pos = q * 4;
+        const int b = (int)(((unsigned)pos * c.zinv) >> 20);
+        x4[k4 + q] = parity_bytes4(s, c.nw, b, pos - b * c.z);
+    }
 }
 
 __global__ void __launch_bounds__(32 * kEncWarps)
@@ -172,16 +175,18 @@ framegen_kernel(CodeDesc c, FramegenArgs a)
             const uint32_t w = s.U[j >> 5] >> (j & 31);
             x4[j >> 2] = (w & 1u) | ((w & 2u) << 7) | ((w & 4u) << 14) | ((w & 8u) << 21);
         }
-        for (int b = 0; b < c.mb; b++)
-            for (int r = lane * 4; r < c.z; r += 128)
-                x4[(c.k + b * c.z + r) >> 2] = parity_bytes4(s, c.nw, b, r);
+        for (int q = lane; q < c.m >> 2; q += 32) {
+            const int pos = q * 4;
+            const int b = (int)(((unsigned)pos * c.zinv) >> 20);
+            x4[(c.k >> 2) + q] = parity_bytes4(s, c.nw, b, pos - b * c.z);
+        }
     }
     if (a.llr) {
         const uint32_t* U = s.U;
         const uint32_t* out = s.out;
         emit_llr(c, a, f, g, scale, sigma, lane, [&](int j) -> uint32_t {
             if (j < c.k) return U[j >> 5] >> (j & 31);
-            const int p = j - c.k, b = p / c.z, r = p - b * c.z;
+            const int p = j - c.k, b = (int)(((unsigned)p * c.zinv) >> 20), r = p - b * c.z;
             return out[b * c.nw + (r >> 5)] >> (r & 31);
         });
     }

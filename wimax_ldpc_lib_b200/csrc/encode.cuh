@@ -31,9 +31,12 @@ namespace wldpc {
 /* Runtime description of one (rate, z) code, passed by value to kernels. */
 struct CodeDesc {
     int rate, z, mb, kb, n, k, m, D, X, nblk, nw;   /* nw = words per z-bit block */
+    unsigned zinv;                       /* ceil(2^20 / z): p / z = (p * zinv) >> 20 for p <= 12 z */
     unsigned char row_start[kMaxMb + 1];
     unsigned char col[96];
     unsigned char shift[96];
+    unsigned char info_start[kMaxMb + 1];   /* the info-column blocks of each row: */
+    uint32_t info_blk[96];                  /* col * z | shift << 16 */
 };
 
 inline CodeDesc make_code_desc(int rate, int z)
@@ -49,18 +52,22 @@ inline CodeDesc make_code_desc(int rate, int z)
     c.D = D_of(rate, z);
     c.X = kX[rate];
     c.nw = (z + 31) / 32;
-    int b = 0;
+    c.zinv = ((1u << 20) + (unsigned)z - 1u) / (unsigned)z;
+    int b = 0, q = 0;
     for (int i = 0; i < c.mb; i++) {
         c.row_start[i] = (unsigned char)b;
+        c.info_start[i] = (unsigned char)q;
         for (int j = 0; j < kNB; j++) {
             const int p = kBase[rate][i][j];
             if (p < 0) continue;
             c.col[b] = (unsigned char)j;
             c.shift[b] = (unsigned char)shift_rule(rate, p, z);
+            if (j < c.kb) c.info_blk[q++] = (uint32_t)(j * z) | ((uint32_t)c.shift[b] << 16);
             b++;
         }
     }
     c.row_start[c.mb] = (unsigned char)b;
+    c.info_start[c.mb] = (unsigned char)q;
     c.nblk = b;
     return c;
 }
@@ -107,13 +114,12 @@ __device__ __forceinline__ void warp_encode_parity(const CodeDesc& c, EncScratch
     for (int p = lane; p < c.mb * nw; p += 32) {
         const int i = div_nw(p, nw), w = p - i * nw;
         uint32_t v = 0;
-        for (int b = c.row_start[i]; b < c.row_start[i + 1]; b++) {
-            const int col = c.col[b];
-            if (col >= c.kb) continue;
-            int t = 32 * w + c.shift[b];
+        for (int q = c.info_start[i]; q < c.info_start[i + 1]; q++) {
+            const uint32_t cs = c.info_blk[q];   /* one constant load per block */
+            int t = 32 * w + (int)(cs >> 16);
             t = t >= z ? t - z : t;
             t = t >= z ? t - z : t;
-            v ^= rot32(s.U, col * z, z, t);
+            v ^= rot32(s.U, (int)(cs & 0xffffu), z, t);
         }
         const int rem = z - 32 * w;
         if (rem < 32) v &= (1u << rem) - 1u;
