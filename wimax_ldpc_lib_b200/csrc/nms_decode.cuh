@@ -241,15 +241,16 @@ __device__ __forceinline__ void tdmp_layer_edges(At&& at, float (&Mr)[NB])
         const float l = __fsub_rn(*at(E), Mr[b0 + e]);
         L[e] = l;
         LC[e] = __float_as_uint(canon(l));
-        sgn = __funnelshift_l(LC[e], sgn, 1);
+        sgn ^= LC[e];   /* bit 31: parity of the negative L */
     });
     two_min_abs<0, d>(L, m1, m2);
     m1 = fminf(m1, 10000.0f);
     m2 = fminf(m2, 10000.0f);
-    const uint32_t flip = (uint32_t)((d & 1) ^ (__popc(sgn) & 1));
+    const uint32_t fb = (sgn ^ ((uint32_t)(d & 1) << 31)) & 0x80000000u;
     const double D1 = __dmul_rn((double)m1, 0.815), D2 = __dmul_rn((double)m2, 0.815);
-    const float f1 = __double2float_rn(D1), f2 = __double2float_rn(D2);
-    const uint32_t fb = flip << 31;
+    /* the magnitudes carry the row's sign flip already (they are >= +0), so
+     * edge e's sign is one XOR with the sign bit of its L */
+    const uint32_t f1 = __float_as_uint(__double2float_rn(D1)) | fb, f2 = __float_as_uint(__double2float_rn(D2)) | fb;
     const int h1 = __double2hiint(D1) ^ (int)fb, l1 = __double2loint(D1);
     const int h2 = __double2hiint(D2) ^ (int)fb, l2 = __double2loint(D2);
     static_for<d>([&](auto E) {
@@ -261,18 +262,22 @@ __device__ __forceinline__ void tdmp_layer_edges(At&& at, float (&Mr)[NB])
         const int lo = is_min ? l2 : l1;
         hi ^= (int)sb;
         *at(E) = __double2float_rn(__dadd_rn((double)l, __hiloint2double(hi, lo)));
-        Mr[b0 + e] = __uint_as_float(__float_as_uint(is_min ? f2 : f1) | (sb ^ fb));
+        Mr[b0 + e] = __uint_as_float((is_min ? f2 : f1) ^ sb);
     });
 }
 
 /* Which message layout the specialised normalized min-sum decoder uses: one
- * float per edge in registers where that measured faster (rate 1/2 at z = 48
- * and 96: +4% and +7%; rate 2/3B at z = 96: +3%; it needs 128-158 registers,
- * fewer resident CTAs, and lost 1-9% at the other rates and at z = 24),
- * else the compressed per-row form (3 registers per layer). */
+ * float per edge in registers where that measured more than 1% faster on a
+ * B200 (all 114 codes timed both ways, outputs identical: 36 codes, by up to
+ * 24%), else the compressed per-row form (3 registers per layer), which was
+ * up to 1.6x faster on the others: the per-edge form needs 128-168 registers
+ * and so fewer resident CTAs. Bit (z - 24) / 4 of kEdgeMsgZ[rate]. */
+constexpr uint32_t kEdgeMsgZ[kRates] = {0x44f55u, 0x44644u, 0x44654u, 0x40c44u, 0x40cc4u, 0x40004u};
+
 constexpr bool tdmp_edge_messages(int rate, int z, int mode)
 {
-    return mode == kNms && ((rate == 0 && (z == 48 || z == 96)) || (rate == 2 && z == 96));
+    return mode == kNms && z >= kZMin && z <= kZMax && z % kZStep == 0 &&
+           ((kEdgeMsgZ[rate] >> ((z - kZMin) / kZStep)) & 1u) != 0;
 }
 
 /* Syndrome of the thread's rows over all layers: 1 if any row fails. The
