@@ -22,6 +22,8 @@ and is no worse than the plain decoder's, else the plain one's.
              also reports its own e2e, with and without the posterior
   roofline   the decode kernel against the measured HBM copy bandwidth, and
              the issue-slot roofline that actually binds it
+  decoders.*.with_posterior  each decoder again with the float32 posterior
+             written back (9n bytes per frame instead of 5n)
   cpu_baseline  the reference's own OpenMP decoder (compiled from its sources)
              on this machine's host cores, on a bounded sample of the workload
   config1    rate 5/6 z=96, 262144 frames at 4 dB, the three decoders
@@ -398,6 +400,18 @@ def run_ours(args):
     sampler.start()
     time.sleep(0.3)
     results = {name: measure(dec, info, k, frames) for name, dec in decoders.items()}
+    # the same decodes with the posterior written back as float32 (the
+    # reference's decode(float*) leaves it in rx): 9n algorithmic bytes per frame
+    post = torch.empty_like(llr)
+    for name, dec in decoders.items():
+        ms_p = timed_steps(lambda: dec.decode_device(llr, hard, post, status, stream=stream), args.steps,
+                           args.warmup, stream, ws)
+        ms_p, _ = reduce_step(ms_p, [], ws, dev)
+        results[name]["with_posterior"] = {
+            "ms_per_step": ms_p, "value": frames * ws * k / (ms_p * 1e-3) / 1e9, "unit": "info Gbit/s",
+            "hbm_gbs": frames * 9 * n / (ms_p * 1e-3) / 1e9,
+            "note": "float32 posterior written back: 9n bytes per frame (LLR read, posterior and hard bits written)"}
+    del post
     clocks = sampler.stop()
     for dec in decoders.values():
         if hasattr(dec, "synchronize"):
@@ -485,6 +499,8 @@ def run_ours(args):
         roofline["issue"] = iss
     for name, r in results.items():
         r["hbm_frac"] = frames * 5 * n / (r["ms_per_step"] * 1e-3) / 1e9 / peak
+        if "with_posterior" in r:
+            r["with_posterior"]["hbm_frac"] = r["with_posterior"]["hbm_gbs"] / peak
         ir = issue_roofline(PROFILES[name].format(r=12, z=Z), frames, r["ms_per_step"], clocks, sms)
         r["issue_frac"] = ir["frac"] if ir else None
 
