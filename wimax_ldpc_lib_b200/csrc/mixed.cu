@@ -174,13 +174,13 @@ static int mixed_enqueue(wldpc_mixed* h, const uint8_t* variant, const long long
     a.max_iter = (int)h->max_iter;
     const int T = h->threads;
     const int ti = T == 96 ? 0 : 1;
-    const int smem = mixed_smem_bytes(T, h->layout);
     if (cudaGetLastError() != cudaSuccess) return WLDPC_ERR_CUDA;
     if (h->launch == WLDPC_MIXED_SERIAL) {
         /* one rate after another on st, each grid with the whole GPU */
         for (int rate = 0; rate < kRates; rate++) {
             memcpy(a.codes, h->codes + rate * kNumZ, sizeof(a.codes));
-            mixed_kernel(ti, h->layout, rate)<<<h->sms * h->per_sm[ti][h->layout][rate], T, smem, st>>>(a);
+            mixed_kernel(ti, h->layout, rate)<<<h->sms * h->per_sm[ti][h->layout][rate], T,
+                                               mixed_smem_bytes(T, h->layout, rate), st>>>(a);
             if (cudaGetLastError() != cudaSuccess) return WLDPC_ERR_CUDA;
         }
         return WLDPC_OK;
@@ -198,7 +198,7 @@ static int mixed_enqueue(wldpc_mixed* h, const uint8_t* variant, const long long
             break;
         }
         memcpy(a.codes, h->codes + rate * kNumZ, sizeof(a.codes));
-        k<<<h->sms * per_sm, T, smem, h->rs[rate]>>>(a);
+        k<<<h->sms * per_sm, T, mixed_smem_bytes(T, h->layout, rate), h->rs[rate]>>>(a);
         if (cudaGetLastError() != cudaSuccess) rc = WLDPC_ERR_CUDA;
         if (cudaEventRecord(h->ev_join[rate], h->rs[rate]) != cudaSuccess ||
             cudaStreamWaitEvent(st, h->ev_join[rate], 0) != cudaSuccess) {
@@ -251,7 +251,7 @@ int wldpc_mixed_create(unsigned max_iter, wldpc_mixed** out)
         for (int layout = 0; layout < 2; layout++)
             for (int rate = 0; rate < kRates; rate++) {
                 const int T = kThreadChoices[ti];
-                const int smem = mixed_smem_bytes(T, layout);
+                const int smem = mixed_smem_bytes(T, layout, rate);
                 const MixedKernel k = mixed_kernel(ti, layout, rate);
                 int per = 0;
                 if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||

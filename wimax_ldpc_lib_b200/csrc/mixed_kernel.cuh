@@ -43,12 +43,14 @@ struct MixedOcc {
     static constexpr int MIN_CTAS = THREADS == 96 ? 8 : 4;
 };
 
-/* dynamic shared memory of a CTA: the posteriors (24 floats per thread), the
- * 16-bit address table (96 blocks per thread) and, in the shared layout, the
- * messages (3 words per layer per thread) */
-constexpr int mixed_smem_bytes(int threads, int layout)
+/* dynamic shared memory of a CTA of the rate's kernel: the posteriors (24
+ * floats per thread), the 16-bit address table (one entry per non-zero block
+ * per thread) and, in the shared layout, the messages (3 words per layer per
+ * thread). Sized per rate, so 8 CTAs of 96 threads fit an SM's 228 KB. */
+constexpr int mixed_smem_bytes(int threads, int layout, int rate)
 {
-    return 24 * threads * 4 + 96 * threads * 2 + (layout == kMsgShared ? 3 * kMaxMb * threads * 4 : 0);
+    return 24 * threads * 4 + num_blocks(rate) * threads * 2 +
+           (layout == kMsgShared ? 3 * kMb[rate] * threads * 4 : 0);
 }
 
 struct MixedCtl {
@@ -98,12 +100,13 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
     }
 
     /* messages: registers (every index a compile-time constant), or shared
-     * memory after the address table, [3][kMaxMb][THREADS] */
+     * memory after the address table, [3][MB][THREADS] */
     float rM1[MB], rM2[MB];
     uint32_t rNEG[MB];
-    float* const sM1 = smem + 24 * THREADS + 48 * THREADS + tid;
-    float* const sM2 = sM1 + kMaxMb * THREADS;
-    uint32_t* const sNEG = reinterpret_cast<uint32_t*>(sM2 + kMaxMb * THREADS);
+    static_assert(THREADS % 2 == 0, "the address table must end on a word boundary");
+    float* const sM1 = smem + 24 * THREADS + NBLK * THREADS / 2 + tid;
+    float* const sM2 = sM1 + MB * THREADS;
+    uint32_t* const sNEG = reinterpret_cast<uint32_t*>(sM2 + MB * THREADS);
 
     int frame = -1, iters = 0;
     long long off = 0;
