@@ -92,6 +92,11 @@ struct wldpc_decoder {
     unsigned* err = nullptr;   /* device error word */
     DevBuf llr, hard, status, bits;
     DevBuf pllr[kHostStages], phard[kHostStages], pstatus[kHostStages];
+    /* one frame per call: a device block [posterior 4n | hard n | status 4]
+     * and its pinned host image (+ the error word), so a call is one copy in,
+     * one launch and two copies out, none of them through pageable memory */
+    DevBuf one;
+    unsigned char* one_host = nullptr;
 };
 
 struct wldpc_encoder {
@@ -213,6 +218,7 @@ int wldpc_decoder_destroy(wldpc_decoder* d)
         }
     if (d->stream) cudaStreamDestroy(d->stream);
     if (d->err) cudaFree(d->err);
+    if (d->one_host) cudaFreeHost(d->one_host);
     delete d;
     return WLDPC_OK;
 }
@@ -284,23 +290,48 @@ int wldpc_decoder_synchronize(wldpc_decoder* d)
     return read_err(d);
 }
 
-static int decode_frames_host(wldpc_decoder* d, float* rx, int8_t* decoded, int32_t* status_host,
-                              size_t frames)
+/* One frame (the reference's per-frame decode(float*)): the caller's buffers
+ * are usually pageable, so the frame goes through the decoder's pinned block
+ * by host memcpy and crosses PCIe in one copy each way. */
+static int decode_one_host(wldpc_decoder* d, float* rx, int8_t* decoded, int32_t* status_host)
 {
     const size_t n = (size_t)d->code.n;
+    const size_t block = 5 * n + 4;   /* 4n and 5n are multiples of 16 (n = 24 z, z a multiple of 4) */
     int rc;
-    if ((rc = d->llr.reserve(frames * n * 4)) || (rc = d->hard.reserve(frames * n)) ||
-        (rc = d->status.reserve(frames * 4)))
+    if ((rc = d->one.reserve(block))) return rc;
+    if (!d->one_host) {
+        void* h = nullptr;
+        if (cudaHostAlloc(&h, block + 4, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return WLDPC_ERR_CUDA;
+        }
+        d->one_host = (unsigned char*)h;
+    }
+    unsigned char* dev = (unsigned char*)d->one.p;
+    unsigned char* host = d->one_host;
+    unsigned* err_host = (unsigned*)(host + block);
+    memcpy(host, rx, n * 4);
+    CU(cudaMemcpyAsync(dev, host, n * 4, cudaMemcpyHostToDevice, d->stream));
+    if ((rc = decode_launch(d, (const float*)dev, (int8_t*)(dev + 4 * n), (float*)dev, (int32_t*)(dev + 5 * n), 1,
+                            d->stream))) {
+        cudaStreamSynchronize(d->stream);
         return rc;
-    CU(cudaMemcpyAsync(d->llr.p, rx, frames * n * 4, cudaMemcpyHostToDevice, d->stream));
-    if ((rc = decode_launch(d, (const float*)d->llr.p, (int8_t*)d->hard.p, (float*)d->llr.p,
-                            (int32_t*)d->status.p, frames, d->stream)))
-        return rc;
-    CU(cudaMemcpyAsync(rx, d->llr.p, frames * n * 4, cudaMemcpyDeviceToHost, d->stream));
-    CU(cudaMemcpyAsync(decoded, d->hard.p, frames * n, cudaMemcpyDeviceToHost, d->stream));
-    CU(cudaMemcpyAsync(status_host, d->status.p, frames * 4, cudaMemcpyDeviceToHost, d->stream));
+    }
+    if (cudaMemcpyAsync(host, dev, block, cudaMemcpyDeviceToHost, d->stream) != cudaSuccess ||
+        cudaMemcpyAsync(err_host, d->err, 4, cudaMemcpyDeviceToHost, d->stream) != cudaSuccess) {
+        cudaStreamSynchronize(d->stream);
+        cudaGetLastError();
+        return WLDPC_ERR_CUDA;
+    }
     CU(cudaStreamSynchronize(d->stream));
-    return read_err(d);
+    if (*err_host) {
+        CU(cudaMemset(d->err, 0, sizeof(unsigned)));
+        return WLDPC_ERR_TIMEOUT;
+    }
+    memcpy(rx, host, n * 4);
+    memcpy(decoded, host + 4 * n, n);
+    memcpy(status_host, host + 5 * n, 4);
+    return WLDPC_OK;
 }
 
 static unsigned ref_return(const wldpc_decoder* d, int32_t status)
@@ -313,7 +344,7 @@ int wldpc_decoder_decode(wldpc_decoder* d, float* rx_codeword, int8_t* decoded, 
 {
     if (!d || !rx_codeword || !decoded) return WLDPC_ERR_ARG;
     int32_t st = 0;
-    int rc = decode_frames_host(d, rx_codeword, decoded, &st, 1);
+    int rc = decode_one_host(d, rx_codeword, decoded, &st);
     if (rc) return rc;
     if (num_errors) *num_errors = ref_return(d, st);
     if (iterations) *iterations = st & 0xffff;
