@@ -31,8 +31,14 @@ def test_staging_wait_timeout_is_reported_and_the_next_call_is_clean(wl, cuda, o
     with pytest.raises(wl.LdpcError) as e:      # the synchronous host path reports it too
         dec.decode_host(llr)
     assert e.value.code == wl.ERR_TIMEOUT
+    with pytest.raises(wl.LdpcError) as e:      # and the single-frame path (pinned block)
+        dec.decode(llr[0])
+    assert e.value.code == wl.ERR_TIMEOUT
 
     dec.set_wait_limit(wl.WAIT_LIMIT_DEFAULT_US)
+    p1, d1, ne1, it1 = dec.decode(llr[0])       # single frame after a timeout: clean and exact
+    assert (p1.view(np.uint32) == po[0].view(np.uint32)).all() and (d1 == do[0]).all()
+    assert it1 == io[0] and ne1 == ro[0]
     dec.decode_device(d_llr, hard, None, status)
     dec.synchronize()                           # the error word was cleared: no stale timeout
     cuda.cuda.synchronize()
