@@ -353,12 +353,14 @@ WLDPC_API int wldpc_mixed_decode_device(wldpc_mixed* h, const uint8_t* variant, 
 /* Waits for the handle's work; WLDPC_ERR_ARG if a frame had an invalid code
  * or an offset that is not a multiple of 4 (such frames are not decoded). */
 WLDPC_API int wldpc_mixed_synchronize(wldpc_mixed* h);
-/* The autotuner's knobs: CTA size (96 or 192 threads, which sets the frame
- * slots per CTA to threads / z), where each thread's compressed messages
- * live (registers, or shared memory: fewer registers and more resident CTAs)
+/* The autotuner's knobs: CTA size (96 or 192 threads), expanded rows per
+ * thread (1 or 2, i.e. z or z/2 threads per frame: the frame slots per CTA
+ * are threads * rows / z), where each thread's compressed messages live
+ * (registers, or shared memory: fewer registers and more resident CTAs),
  * frames per work item (1..64) and whether the six per-rate grids run
- * concurrently or one after another. set_config / get_config leave layout
- * and launch policy as they are. */
+ * concurrently or one after another. set_tuning and set_config leave the
+ * rows per thread as they are; set_config / get_config also leave layout and
+ * launch policy. */
 #define WLDPC_MIXED_MSG_REGISTERS 0
 #define WLDPC_MIXED_MSG_SHARED 1
 #define WLDPC_MIXED_CONCURRENT 0
@@ -367,9 +369,12 @@ WLDPC_API int wldpc_mixed_set_tuning(wldpc_mixed* h, int threads, int layout, in
 WLDPC_API int wldpc_mixed_get_tuning(wldpc_mixed* h, int* threads, int* layout, int* chunk, int* launch);
 WLDPC_API int wldpc_mixed_set_config(wldpc_mixed* h, int threads, int chunk);
 WLDPC_API int wldpc_mixed_get_config(wldpc_mixed* h, int* threads, int* chunk);
-/* Times every (threads, layout, chunk, launch) candidate on the given batch
- * (repeats launches each) and keeps the fastest; *best_ms (nullable) gets its
- * time. */
+/* rows = 1 or 2 expanded rows per thread (WLDPC_ERR_ARG otherwise) */
+WLDPC_API int wldpc_mixed_set_rows_per_thread(wldpc_mixed* h, int rows);
+WLDPC_API int wldpc_mixed_get_rows_per_thread(wldpc_mixed* h, int* rows);
+/* Times every (threads, rows per thread, layout, chunk, launch) candidate on
+ * the given batch (repeats launches each) and keeps the fastest; *best_ms
+ * (nullable) gets its time. */
 WLDPC_API int wldpc_mixed_autotune(wldpc_mixed* h, const uint8_t* variant, const int64_t* offset, const float* llr,
                                    int8_t* decoded, size_t frames, int repeats, float* best_ms);
 

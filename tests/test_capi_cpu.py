@@ -118,6 +118,8 @@ def test_argument_checks_of_the_additions(wl):
     assert L.wldpc_mixed_create(10, None) == wl.ERR_ARG
     assert L.wldpc_mixed_destroy(None) == wl.ERR_ARG
     assert L.wldpc_mixed_set_config(None, 96, 32) == wl.ERR_ARG
+    assert L.wldpc_mixed_set_rows_per_thread(None, 1) == wl.ERR_ARG
+    assert L.wldpc_mixed_get_rows_per_thread(None, None) == wl.ERR_ARG
     # allocation-free decode: code, cap and the scratch limit come before any device call
     assert L.wldpc_decode_host_noalloc(0, 100, 10, None, None, None, 1) == wl.ERR_CODE
     assert L.wldpc_decode_host_noalloc(0, 96, 0x10000, None, None, None, 1) == wl.ERR_ARG

@@ -42,12 +42,16 @@ def test_mixed_matches_specialised_decoders(wl, cuda, batch):
     decode_by_code(groups, llr, ref_hard, ref_status)
     mixed = wl.MixedDecoder(10)
     R, S = wl.MIXED_MSG_REGISTERS, wl.MIXED_MSG_SHARED
-    # every CTA size and message layout; chunks from one frame per item to the maximum
+    # every CTA size, rows per thread and message layout; chunks from one
+    # frame per item to the maximum
     C, Q = wl.MIXED_CONCURRENT, wl.MIXED_SERIAL
-    for threads, layout, chunk, launch in [(96, R, 32, C), (96, S, 8, Q), (192, R, 64, Q), (192, S, 16, C),
-                                           (96, R, 1, C), (192, S, 3, Q)]:
+    for threads, layout, chunk, launch, rows in [(96, R, 32, C, 1), (96, S, 8, Q, 1), (192, R, 64, Q, 1),
+                                                 (192, S, 16, C, 1), (96, R, 1, C, 1), (192, S, 3, Q, 1),
+                                                 (96, R, 16, C, 2), (96, S, 64, Q, 2), (192, R, 8, Q, 2),
+                                                 (192, S, 5, C, 2)]:
         mixed.set_tuning(threads, layout, chunk, launch)
-        assert mixed.tuning() == (threads, layout, chunk, launch)
+        mixed.set_rows_per_thread(rows)
+        assert mixed.tuning() == (threads, layout, chunk, launch) and mixed.rows_per_thread() == rows
         for _ in range(2):   # capture, then replay
             hard = torch.zeros(llr.numel(), dtype=torch.int8, device="cuda")
             status = torch.full((frames,), -1, dtype=torch.int32, device="cuda")
@@ -55,8 +59,8 @@ def test_mixed_matches_specialised_decoders(wl, cuda, batch):
             mixed.decode_device(variants, offsets, llr, hard, post, status)
             torch.cuda.synchronize()
             mixed.synchronize()
-            assert torch.equal(hard, ref_hard), (threads, layout, chunk)
-            assert torch.equal(status, ref_status), (threads, layout, chunk)
+            assert torch.equal(hard, ref_hard), (threads, layout, chunk, rows)
+            assert torch.equal(status, ref_status), (threads, layout, chunk, rows)
 
 
 def test_mixed_matches_oracle_sample(wl, cuda, oracle, batch):
@@ -87,6 +91,7 @@ def test_mixed_autotune_and_bad_code(wl, cuda, batch):
     ms = mixed.autotune(variants, offsets, llr, hard, repeats=1)
     threads, layout, chunk, launch = mixed.tuning()
     assert ms > 0 and threads in (96, 192) and layout in (0, 1) and chunk in (8, 16, 32, 64) and launch in (0, 1)
+    assert mixed.rows_per_thread() in (1, 2)
     bad = variants.clone()
     bad[0] = 200
     mixed.decode_device(bad, offsets, llr, hard)
@@ -105,3 +110,5 @@ def test_mixed_autotune_and_bad_code(wl, cuda, batch):
     mixed.synchronize()
     with pytest.raises(wl.LdpcError):
         mixed.set_tuning(96, 0, 65, 0)                     # at most 64 frames per work item
+    with pytest.raises(wl.LdpcError):
+        mixed.set_rows_per_thread(3)                       # one or two rows per thread

@@ -117,6 +117,8 @@ def _lib():
     L.wldpc_mixed_set_config.argtypes = [_p, _i, _i]
     L.wldpc_mixed_get_config.argtypes = [_p, ctypes.POINTER(_i), ctypes.POINTER(_i)]
     L.wldpc_mixed_set_tuning.argtypes = [_p, _i, _i, _i, _i]
+    L.wldpc_mixed_set_rows_per_thread.argtypes = [_p, _i]
+    L.wldpc_mixed_get_rows_per_thread.argtypes = [_p, ctypes.POINTER(_i)]
     L.wldpc_mixed_get_tuning.argtypes = [_p, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i),
                                          ctypes.POINTER(_i)]
     L.wldpc_mixed_autotune.argtypes = [_p, _p, _p, _p, _p, _sz, _i, ctypes.POINTER(ctypes.c_float)]
@@ -385,6 +387,15 @@ class MixedDecoder:
         _check(_lib().wldpc_mixed_get_tuning(self._h, ctypes.byref(t), ctypes.byref(l), ctypes.byref(c),
                                              ctypes.byref(p)), "mixed tuning")
         return t.value, l.value, c.value, p.value
+
+    def set_rows_per_thread(self, rows: int):
+        """1 or 2 expanded rows per thread: z or z/2 threads per frame."""
+        _check(_lib().wldpc_mixed_set_rows_per_thread(self._h, rows), "mixed rows per thread")
+
+    def rows_per_thread(self) -> int:
+        r = _i()
+        _check(_lib().wldpc_mixed_get_rows_per_thread(self._h, ctypes.byref(r)), "mixed rows per thread")
+        return r.value
 
     def autotune(self, variants, offsets, llr, decoded, repeats: int = 3) -> float:
         ms = ctypes.c_float()

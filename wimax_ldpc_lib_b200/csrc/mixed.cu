@@ -106,28 +106,31 @@ inline bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_
 }  // namespace
 
 namespace wldpc {
-/* [threads 96 | 192][layout registers | shared], per rate (mixed_instances.cuh) */
-extern const MixedKernel kMixed_r0[2][2];
-extern const MixedKernel kMixed_r1[2][2];
-extern const MixedKernel kMixed_r2[2][2];
-extern const MixedKernel kMixed_r3[2][2];
-extern const MixedKernel kMixed_r4[2][2];
-extern const MixedKernel kMixed_r5[2][2];
+/* [threads 96 | 192][layout registers | shared][rows per thread 1 | 2], per
+ * rate (mixed_instances.cuh) */
+extern const MixedKernel kMixed_r0[2][2][2];
+extern const MixedKernel kMixed_r1[2][2][2];
+extern const MixedKernel kMixed_r2[2][2][2];
+extern const MixedKernel kMixed_r3[2][2][2];
+extern const MixedKernel kMixed_r4[2][2][2];
+extern const MixedKernel kMixed_r5[2][2][2];
 }  // namespace wldpc
 
-static MixedKernel mixed_kernel(int ti, int layout, int rate)
+static MixedKernel mixed_kernel(int ti, int layout, int rows, int rate)
 {
-    static const MixedKernel (*const t[kRates])[2] = {kMixed_r0, kMixed_r1, kMixed_r2, kMixed_r3, kMixed_r4, kMixed_r5};
-    return t[rate][ti][layout];
+    static const MixedKernel (*const t[kRates])[2][2] = {kMixed_r0, kMixed_r1, kMixed_r2,
+                                                          kMixed_r3, kMixed_r4, kMixed_r5};
+    return t[rate][ti][layout][rows - 1];
 }
 
 struct wldpc_mixed {
     unsigned max_iter;
     int threads = 96, layout = kMsgRegisters, chunk = 16;
+    int rows = 1;                          /* expanded rows per thread: z / rows threads per frame */
     int launch = WLDPC_MIXED_CONCURRENT;   /* the six rate grids: concurrent or one after another */
     MixedCode codes[kVariants];            /* every code, by variant */
     int sms = 148;
-    int per_sm[2][2][kRates] = {};   /* resident CTAs per SM, [96 | 192 threads][layout][rate] */
+    int per_sm[2][2][2][kRates] = {};   /* resident CTAs per SM, [96 | 192 threads][layout][rows - 1][rate] */
     cudaStream_t stream = nullptr;
     cudaStream_t rs[kRates] = {};
     cudaEvent_t ev_in = nullptr, ev_out = nullptr, ev_fork = nullptr, ev_join[kRates] = {};
@@ -139,7 +142,7 @@ struct wldpc_mixed {
     struct Key {
         const void *variant, *offset, *llr, *hard, *post, *status;
         size_t frames;
-        int threads, layout, chunk, launch;
+        int threads, layout, chunk, launch, rows;
         bool operator==(const Key& o) const { return memcmp(this, &o, sizeof(Key)) == 0; }
     } key{};
 };
@@ -179,8 +182,8 @@ static int mixed_enqueue(wldpc_mixed* h, const uint8_t* variant, const long long
         /* one rate after another on st, each grid with the whole GPU */
         for (int rate = 0; rate < kRates; rate++) {
             memcpy(a.codes, h->codes + rate * kNumZ, sizeof(a.codes));
-            mixed_kernel(ti, h->layout, rate)<<<h->sms * h->per_sm[ti][h->layout][rate], T,
-                                               mixed_smem_bytes(T, h->layout, rate), st>>>(a);
+            mixed_kernel(ti, h->layout, h->rows, rate)<<<h->sms * h->per_sm[ti][h->layout][h->rows - 1][rate], T,
+                                                         mixed_smem_bytes(T, h->layout, rate, h->rows), st>>>(a);
             if (cudaGetLastError() != cudaSuccess) return WLDPC_ERR_CUDA;
         }
         return WLDPC_OK;
@@ -191,14 +194,14 @@ static int mixed_enqueue(wldpc_mixed* h, const uint8_t* variant, const long long
      * capture in progress always ends with all its streams joined */
     int rc = WLDPC_OK;
     for (int rate = 0; rate < kRates; rate++) {
-        const MixedKernel k = mixed_kernel(ti, h->layout, rate);
-        const int per_sm = h->per_sm[ti][h->layout][rate];
+        const MixedKernel k = mixed_kernel(ti, h->layout, h->rows, rate);
+        const int per_sm = h->per_sm[ti][h->layout][h->rows - 1][rate];
         if (cudaStreamWaitEvent(h->rs[rate], h->ev_fork, 0) != cudaSuccess) {
             rc = WLDPC_ERR_CUDA;
             break;
         }
         memcpy(a.codes, h->codes + rate * kNumZ, sizeof(a.codes));
-        k<<<h->sms * per_sm, T, mixed_smem_bytes(T, h->layout, rate), h->rs[rate]>>>(a);
+        k<<<h->sms * per_sm, T, mixed_smem_bytes(T, h->layout, rate, h->rows), h->rs[rate]>>>(a);
         if (cudaGetLastError() != cudaSuccess) rc = WLDPC_ERR_CUDA;
         if (cudaEventRecord(h->ev_join[rate], h->rs[rate]) != cudaSuccess ||
             cudaStreamWaitEvent(st, h->ev_join[rate], 0) != cudaSuccess) {
@@ -249,19 +252,20 @@ int wldpc_mixed_create(unsigned max_iter, wldpc_mixed** out)
     /* shared-memory limit and occupancy of every decode kernel, once, outside any capture */
     for (int ti = 0; ti < 2; ti++)
         for (int layout = 0; layout < 2; layout++)
-            for (int rate = 0; rate < kRates; rate++) {
-                const int T = kThreadChoices[ti];
-                const int smem = mixed_smem_bytes(T, layout, rate);
-                const MixedKernel k = mixed_kernel(ti, layout, rate);
-                int per = 0;
-                if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
-                    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, T, smem) != cudaSuccess) {
-                    cudaGetLastError();
-                    delete h;
-                    return WLDPC_ERR_CUDA;
+            for (int rows = 1; rows <= 2; rows++)
+                for (int rate = 0; rate < kRates; rate++) {
+                    const int T = kThreadChoices[ti];
+                    const int smem = mixed_smem_bytes(T, layout, rate, rows);
+                    const MixedKernel k = mixed_kernel(ti, layout, rows, rate);
+                    int per = 0;
+                    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+                        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, T, smem) != cudaSuccess) {
+                        cudaGetLastError();
+                        delete h;
+                        return WLDPC_ERR_CUDA;
+                    }
+                    h->per_sm[ti][layout][rows - 1][rate] = per > 0 ? per : 1;
                 }
-                h->per_sm[ti][layout][rate] = per > 0 ? per : 1;
-            }
     bool ok = true;
     for (int r = 0; r < kRates; r++)
         ok = ok && cudaStreamCreateWithFlags(&h->rs[r], cudaStreamNonBlocking) == cudaSuccess &&
@@ -323,6 +327,20 @@ int wldpc_mixed_get_tuning(wldpc_mixed* h, int* threads, int* layout, int* chunk
     return WLDPC_OK;
 }
 
+int wldpc_mixed_set_rows_per_thread(wldpc_mixed* h, int rows)
+{
+    if (!h || (rows != 1 && rows != 2)) return WLDPC_ERR_ARG;
+    h->rows = rows;
+    return WLDPC_OK;
+}
+
+int wldpc_mixed_get_rows_per_thread(wldpc_mixed* h, int* rows)
+{
+    if (!h || !rows) return WLDPC_ERR_ARG;
+    *rows = h->rows;
+    return WLDPC_OK;
+}
+
 int wldpc_mixed_set_config(wldpc_mixed* h, int threads, int chunk)
 {
     if (!h) return WLDPC_ERR_ARG;
@@ -349,7 +367,7 @@ int wldpc_mixed_decode_device(wldpc_mixed* h, const uint8_t* variant, const int6
         (rc = h->items.reserve(max_items * sizeof(MixedItem))))
         return rc;
     wldpc_mixed::Key key{variant,  offset,     llr,       decoded,  posterior, status,
-                         frames,   h->threads, h->layout, h->chunk, h->launch};
+                         frames,   h->threads, h->layout, h->chunk, h->launch, h->rows};
     const cudaStream_t user = (cudaStream_t)stream;
     if (cudaEventRecord(h->ev_in, user) != cudaSuccess || cudaStreamWaitEvent(h->stream, h->ev_in, 0) != cudaSuccess) {
         cudaGetLastError();
@@ -413,57 +431,62 @@ int wldpc_mixed_autotune(wldpc_mixed* h, const uint8_t* variant, const int64_t* 
     if (!h || repeats < 1) return WLDPC_ERR_ARG;
     static const int chunks[4] = {8, 16, 32, 64};
     float best = 1e30f;
-    int bt = h->threads, bl = h->layout, bc = h->chunk, bp = h->launch;
+    int bt = h->threads, bl = h->layout, bc = h->chunk, bp = h->launch, br = h->rows;
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         cudaGetLastError();
         return WLDPC_ERR_CUDA;
     }
-    /* CTA size x message layout x frames per work item x launch policy, timed
-     * on the caller's batch */
+    auto restore = [&]() {
+        h->threads = bt;
+        h->layout = bl;
+        h->chunk = bc;
+        h->launch = bp;
+        h->rows = br;
+    };
+    /* CTA size x rows per thread x message layout x frames per work item x
+     * launch policy, timed on the caller's batch */
     for (int ti = 0; ti < 2; ti++)
-        for (int layout = 0; layout < 2; layout++)
-            for (int ci = 0; ci < 4; ci++)
-                for (int lp = 0; lp < 2; lp++) {
-                h->threads = kThreadChoices[ti];
-                h->layout = layout;
-                h->chunk = chunks[ci];
-                h->launch = lp;
-                int rc = wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr, frames,
-                                                   h->stream);
-                if (!rc && cudaEventRecord(e0, h->stream) != cudaSuccess) rc = WLDPC_ERR_CUDA;
-                for (int k = 0; k < repeats && !rc; k++)
-                    rc = wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr, frames,
-                                                   h->stream);
-                if (!rc && (cudaEventRecord(e1, h->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
-                    rc = WLDPC_ERR_CUDA;
-                if (rc) {
-                    cudaGetLastError();
-                    cudaEventDestroy(e0);
-                    cudaEventDestroy(e1);
-                    h->threads = bt;
-                    h->layout = bl;
-                    h->chunk = bc;
-                    h->launch = bp;
-                    return rc;
-                }
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                ms /= repeats;
-                if (ms < best) {
-                    best = ms;
-                    bt = h->threads;
-                    bl = h->layout;
-                    bc = h->chunk;
-                    bp = h->launch;
-                }
-                }
+        for (int rows = 1; rows <= 2; rows++)
+            for (int layout = 0; layout < 2; layout++)
+                for (int ci = 0; ci < 4; ci++)
+                    for (int lp = 0; lp < 2; lp++) {
+                        h->threads = kThreadChoices[ti];
+                        h->rows = rows;
+                        h->layout = layout;
+                        h->chunk = chunks[ci];
+                        h->launch = lp;
+                        int rc = wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr,
+                                                           frames, h->stream);
+                        if (!rc && cudaEventRecord(e0, h->stream) != cudaSuccess) rc = WLDPC_ERR_CUDA;
+                        for (int k = 0; k < repeats && !rc; k++)
+                            rc = wldpc_mixed_decode_device(h, variant, offset, llr, decoded, nullptr, nullptr,
+                                                           frames, h->stream);
+                        if (!rc && (cudaEventRecord(e1, h->stream) != cudaSuccess ||
+                                    cudaEventSynchronize(e1) != cudaSuccess))
+                            rc = WLDPC_ERR_CUDA;
+                        if (rc) {
+                            cudaGetLastError();
+                            cudaEventDestroy(e0);
+                            cudaEventDestroy(e1);
+                            restore();
+                            return rc;
+                        }
+                        float ms = 0.f;
+                        cudaEventElapsedTime(&ms, e0, e1);
+                        ms /= repeats;
+                        if (ms < best) {
+                            best = ms;
+                            bt = h->threads;
+                            bl = h->layout;
+                            bc = h->chunk;
+                            bp = h->launch;
+                            br = h->rows;
+                        }
+                    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    h->threads = bt;
-    h->layout = bl;
-    h->chunk = bc;
-    h->launch = bp;
+    restore();
     if (best_ms) *best_ms = best;
     return wldpc_mixed_synchronize(h);
 }

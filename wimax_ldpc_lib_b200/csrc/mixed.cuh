@@ -7,19 +7,20 @@
  *   1. binning (mixed_count / mixed_plan / mixed_scatter): frames are
  *      grouped by code (variant = rate * 19 + z index) and cut into work
  *      items of at most `chunk` frames of one code;
- *   2. mixed_decode_kernel<rate, threads, layout> (mixed_kernel.cuh): one
- *      persistent grid per rate, the six launched concurrently or one after
- *      another; each CTA takes work items of its rate from that rate's
- *      counter. The CTA runs G = threads / z frame slots in lockstep (z a
- *      run-time value, edge addresses from a per-item shared-memory table)
+ *   2. mixed_decode_kernel<rate, threads, layout, rows> (mixed_kernel.cuh):
+ *      one persistent grid per rate, the six launched concurrently or one
+ *      after another; each CTA takes work items of its rate from that rate's
+ *      counter. The CTA runs G = threads * rows / z frame slots in lockstep
+ *      (rows = 1 or 2 expanded rows per thread; z a run-time value, edge
+ *      addresses from a per-item shared-memory table)
  *      and refills a slot with the item's next frame (one bulk copy) as soon
  *      as its frame converges or reaches the cap (early-exit compaction). A
  *      refilled frame gets its initial syndrome check before its first
  *      iteration, as in the reference (reference lib/ldpc_decoder.cc:127-139).
  * The binning kernels and the six decode grids (forked onto six streams) are
- * captured in one CUDA graph, so a batch is one graph launch. CTA size,
- * message layout (registers or shared memory) and chunk are picked by the
- * handle's autotuner.
+ * captured in one CUDA graph, so a batch is one graph launch. CTA size, rows
+ * per thread (threads per z), message layout (registers or shared memory),
+ * chunk and launch policy are picked by the handle's autotuner.
  */
 #ifndef WLDPC_MIXED_CUH
 #define WLDPC_MIXED_CUH
@@ -32,7 +33,7 @@
 namespace wldpc {
 
 constexpr int kVariants = kRates * kNumZ;   /* 114 */
-constexpr int kMixedMaxSlots = 8;          /* frames per CTA: 192 threads / z = 24 */
+constexpr int kMixedMaxSlots = 16;         /* frames per CTA: 192 threads x 2 rows / z = 24 */
 constexpr int kMixedMaxChunk = 64;         /* frames per work item */
 
 /* one code of a rate, as the mixed kernel needs it (z at run time) */

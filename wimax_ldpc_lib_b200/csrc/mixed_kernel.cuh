@@ -9,16 +9,18 @@
  * (ncu: 10 no_instruction stalls per issue, issue 16% active) and ran 1.7x
  * slower on the mixed batch.
  *
- * Within an item the CTA runs G = THREADS / z frame slots in lockstep, one
- * thread per expanded row, and refills a slot as soon as its frame converges
- * or reaches the cap (early-exit compaction). A refilled frame arrives by one
+ * Within an item the CTA runs G = THREADS * RPT / z frame slots in lockstep,
+ * z / RPT threads per frame (threads per z: RPT = 1 or 2 expanded rows per
+ * thread; a thread's two rows are r and r + z/2, two independent chains of
+ * the same layer), and refills a slot as soon as its frame converges or
+ * reaches the cap (early-exit compaction). A refilled frame arrives by one
  * cp.async.bulk copy (TMA, no multicast) completed on the slot's mbarrier,
  * and gets its initial syndrome check before its first iteration (reference
  * lib/ldpc_decoder.cc:127-139). The item's frame list and offsets are staged
  * in shared memory at its start, so a refill reads no global memory.
  *
  * LAYOUT selects where a thread's compressed messages (M1, M2, NEG per
- * layer) live: in registers, or in shared memory. The arithmetic is the
+ * layer and row) live: in registers, or in shared memory. The arithmetic is the
  * plain normalized min-sum of tdmp_layer(), bit-exact with the reference.
  *
  * Every mbarrier wait is bounded: on expiry the kernel records
@@ -35,22 +37,25 @@ enum MixedLayout : int { kMsgRegisters = 0, kMsgShared = 1 };
 
 using MixedKernel = void (*)(const MixedArgs);
 
-/* resident CTAs per SM the register allocation is sized for (80 registers
- * per thread; the kernel is latency-bound, so resident warps pay more than
- * the few spills of the rate-5/6 kernel cost) */
-template <int THREADS>
+/* resident CTAs per SM the register allocation is sized for. One row per
+ * thread: 80 registers (the kernel is latency-bound, so resident warps pay
+ * more than the few spills of the rate-5/6 kernel cost), and shared memory
+ * fits as many CTAs. Two rows per thread: twice the shared memory per
+ * thread, so half the CTAs fit, which leaves up to 168 registers. */
+template <int THREADS, int RPT>
 struct MixedOcc {
-    static constexpr int MIN_CTAS = THREADS == 96 ? 8 : 4;
+    static constexpr int MIN_CTAS = (THREADS == 96 ? 8 : 4) / RPT;
 };
 
 /* dynamic shared memory of a CTA of the rate's kernel: the posteriors (24
- * floats per thread), the 16-bit address table (one entry per non-zero block
- * per thread) and, in the shared layout, the messages (3 words per layer per
- * thread). Sized per rate, so 8 CTAs of 96 threads fit an SM's 228 KB. */
-constexpr int mixed_smem_bytes(int threads, int layout, int rate)
+ * floats per row), the 16-bit address table (one entry per non-zero block
+ * per row) and, in the shared layout, the messages (3 words per layer per
+ * row); RPT rows per thread. Sized per rate, so 8 CTAs of 96 threads (one
+ * row each) fit an SM's 228 KB. */
+constexpr int mixed_smem_bytes(int threads, int layout, int rate, int rpt)
 {
-    return 24 * threads * 4 + num_blocks(rate) * threads * 2 +
-           (layout == kMsgShared ? 3 * kMb[rate] * threads * 4 : 0);
+    return (24 * threads * 4 + num_blocks(rate) * threads * 2 +
+            (layout == kMsgShared ? 3 * kMb[rate] * threads * 4 : 0)) * rpt;
 }
 
 struct MixedCtl {
@@ -64,28 +69,31 @@ struct MixedCtl {
     int item;
 };
 
-template <int R, int THREADS, int LAYOUT>
+template <int R, int THREADS, int LAYOUT, int RPT>
 __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem item, float* smem, MixedCtl& S,
                                            uint64_t* bar)
 {
+    static_assert(RPT == 1 || RPT == 2, "one or two rows per thread");
     constexpr int MB = kMb[R];
     constexpr int NBLK = num_blocks(R);
     const MixedCode& code = a.codes[item.variant - R * kNumZ];
     const int z = code.z, n = code.n;
-    const int G = THREADS / z;
+    const int zt = z / RPT;             /* threads per frame (z is a multiple of 4) */
+    const int G = THREADS / zt;
     const int tid = threadIdx.x;
-    const int g = tid / z;
-    const int r = tid - g * z;
+    const int g = tid / zt;
+    const int r = tid - g * zt;         /* rows r + k * zt, k < RPT */
     const bool in_slot = g < G;
     float* const P = smem + (in_slot ? g : 0) * n;
-    unsigned short* const A = reinterpret_cast<unsigned short*>(smem + 24 * THREADS);
-    /* this thread's edge addresses for the item's code, [block][thread] */
-    for (int b = 0; b < NBLK; b++) {
-        int t = r + (int)code.shift[b];
-        t = t >= z ? t - z : t;
-        A[b * THREADS + tid] = in_slot ? (unsigned short)(code.colz[b] + t) : (unsigned short)0;
-    }
-    auto addr = [&](int b) -> int { return A[b * THREADS + tid]; };
+    unsigned short* const A = reinterpret_cast<unsigned short*>(smem + 24 * THREADS * RPT);
+    /* this thread's edge addresses for the item's code, [row k][block][thread] */
+    for (int k = 0; k < RPT; k++)
+        for (int b = 0; b < NBLK; b++) {
+            int t = r + k * zt + (int)code.shift[b];
+            t = t >= z ? t - z : t;
+            A[(k * NBLK + b) * THREADS + tid] = in_slot ? (unsigned short)(code.colz[b] + t) : (unsigned short)0;
+        }
+    auto addr = [&](int k, int b) -> int { return A[(k * NBLK + b) * THREADS + tid]; };
     /* the item's frame list and offsets, one per thread */
     if (tid < item.count) {
         const int f = a.perm[item.start + tid];
@@ -100,13 +108,16 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
     }
 
     /* messages: registers (every index a compile-time constant), or shared
-     * memory after the address table, [3][MB][THREADS] */
-    float rM1[MB], rM2[MB];
-    uint32_t rNEG[MB];
+     * memory after the address table, [row k][3][MB][THREADS] */
+    float rM1[RPT][MB], rM2[RPT][MB];
+    uint32_t rNEG[RPT][MB];
     static_assert(THREADS % 2 == 0, "the address table must end on a word boundary");
-    float* const sM1 = smem + 24 * THREADS + NBLK * THREADS / 2 + tid;
-    float* const sM2 = sM1 + MB * THREADS;
-    uint32_t* const sNEG = reinterpret_cast<uint32_t*>(sM2 + MB * THREADS);
+    float* const sM = smem + 24 * THREADS * RPT + NBLK * THREADS * RPT / 2 + tid;
+    auto sM1 = [&](int k, int i) -> float& { return sM[(k * 3 * MB + i) * THREADS]; };
+    auto sM2 = [&](int k, int i) -> float& { return sM[(k * 3 * MB + MB + i) * THREADS]; };
+    auto sNEG = [&](int k, int i) -> uint32_t& {
+        return reinterpret_cast<uint32_t*>(sM)[(k * 3 * MB + 2 * MB + i) * THREADS];
+    };
 
     int frame = -1, iters = 0;
     long long off = 0;
@@ -141,18 +152,20 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
                 iters = 0;
                 need_check = true;
                 if (!mbar_wait_bounded(&bar[g], (S.phase >> g) & 1u)) atomicOr(&S.abort, 1u);
-                static_for<MB>([&](auto I) {
-                    constexpr int i = decltype(I)::value;
-                    if constexpr (LAYOUT == kMsgRegisters) {
-                        rM1[i] = 0.0f;
-                        rM2[i] = 0.0f;
-                        rNEG[i] = 0u;
-                    } else {
-                        sM1[i * THREADS] = 0.0f;
-                        sM2[i * THREADS] = 0.0f;
-                        sNEG[i * THREADS] = 0u;
-                    }
-                });
+#pragma unroll
+                for (int k = 0; k < RPT; k++)
+                    static_for<MB>([&](auto I) {
+                        constexpr int i = decltype(I)::value;
+                        if constexpr (LAYOUT == kMsgRegisters) {
+                            rM1[k][i] = 0.0f;
+                            rM2[k][i] = 0.0f;
+                            rNEG[k][i] = 0u;
+                        } else {
+                            sM1(k, i) = 0.0f;
+                            sM2(k, i) = 0.0f;
+                            sNEG(k, i) = 0u;
+                        }
+                    });
             }
             __syncthreads();
             if (S.abort) break;
@@ -161,9 +174,12 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
 
         /* 2. syndrome of the slots loaded or iterated since their last check */
         if (in_slot && frame >= 0 && need_check) {
-            const unsigned fail = tdmp_rows_fail<R>([&](auto I, auto E) {
-                return P + addr(block_index(R, decltype(I)::value, decltype(E)::value));
-            });
+            unsigned fail = 0;
+#pragma unroll
+            for (int k = 0; k < RPT; k++)
+                fail |= tdmp_rows_fail<R>([&](auto I, auto E) {
+                    return P + addr(k, block_index(R, decltype(I)::value, decltype(E)::value));
+                });
             if (fail) atomicOr(&S.fail, 1u << g);
         }
         __syncthreads();
@@ -174,8 +190,8 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
             const bool failed = (S.fail >> g) & 1u;
             if (!failed || iters >= a.max_iter) {
 #pragma unroll
-                for (int s = 0; s < 6; s++) {
-                    const int v = r + s * z;                  /* float4 group of the frame */
+                for (int s = 0; s < 6 * RPT; s++) {
+                    const int v = r + s * zt;                 /* float4 group of the frame (6z of them) */
                     const float4 p = reinterpret_cast<const float4*>(P)[v];
                     const uint32_t w = (p.x >= 0.0f ? 1u : 0u) | (p.y >= 0.0f ? 1u << 8 : 0u) |
                                        (p.z >= 0.0f ? 1u << 16 : 0u) | (p.w >= 0.0f ? 1u << 24 : 0u);
@@ -213,19 +229,25 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
             constexpr int i = decltype(I)::value;
             constexpr int d = layer_degree(R, i);
             if (active) {
-                /* the layer's edge addresses, loaded once for both passes */
-                int ad[d];
-                static_for<d>([&](auto E) { ad[decltype(E)::value] = addr(block_index(R, i, decltype(E)::value)); });
-                auto at = [&](auto E) { return P + ad[decltype(E)::value]; };
-                if constexpr (LAYOUT == kMsgRegisters) {
-                    tdmp_layer<R, i, kNms>(at, rM1[i], rM2[i], rNEG[i]);
-                } else {
-                    float a1 = sM1[i * THREADS], a2 = sM2[i * THREADS];
-                    uint32_t ng = sNEG[i * THREADS];
-                    tdmp_layer<R, i, kNms>(at, a1, a2, ng);
-                    sM1[i * THREADS] = a1;
-                    sM2[i * THREADS] = a2;
-                    sNEG[i * THREADS] = ng;
+                /* the layer's rows (independent chains), each with its edge
+                 * addresses loaded once for both passes */
+#pragma unroll
+                for (int k = 0; k < RPT; k++) {
+                    int ad[d];
+                    static_for<d>([&](auto E) {
+                        ad[decltype(E)::value] = addr(k, block_index(R, i, decltype(E)::value));
+                    });
+                    auto at = [&](auto E) { return P + ad[decltype(E)::value]; };
+                    if constexpr (LAYOUT == kMsgRegisters) {
+                        tdmp_layer<R, i, kNms>(at, rM1[k][i], rM2[k][i], rNEG[k][i]);
+                    } else {
+                        float a1 = sM1(k, i), a2 = sM2(k, i);
+                        uint32_t ng = sNEG(k, i);
+                        tdmp_layer<R, i, kNms>(at, a1, a2, ng);
+                        sM1(k, i) = a1;
+                        sM2(k, i) = a2;
+                        sNEG(k, i) = ng;
+                    }
                 }
             }
             __syncthreads();
@@ -249,8 +271,8 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
 
 /* One persistent grid per rate: it takes work items of its rate from its own
  * queue until none are left. */
-template <int R, int THREADS, int LAYOUT>
-__global__ void __launch_bounds__(THREADS, (MixedOcc<THREADS>::MIN_CTAS))
+template <int R, int THREADS, int LAYOUT, int RPT>
+__global__ void __launch_bounds__(THREADS, (MixedOcc<THREADS, RPT>::MIN_CTAS))
 mixed_decode_kernel(const __grid_constant__ MixedArgs a)
 {
     extern __shared__ __align__(128) float smem_mixed[];
@@ -268,7 +290,7 @@ mixed_decode_kernel(const __grid_constant__ MixedArgs a)
         const int k = S.item;
         __syncthreads();
         if (k >= a.num_items[R]) break;
-        if (!mixed_item<R, THREADS, LAYOUT>(a, items[k], smem_mixed, S, bar)) break;
+        if (!mixed_item<R, THREADS, LAYOUT, RPT>(a, items[k], smem_mixed, S, bar)) break;
         __syncthreads();
     }
 }

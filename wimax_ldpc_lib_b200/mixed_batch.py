@@ -90,7 +90,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--out", default=None, help="also write the JSON result to this file")
     ap.add_argument("--sweep", action="store_true", help="time every tuning candidate")
-    ap.add_argument("--tuning", default=None, help="threads,layout,chunk,launch instead of the autotuner")
+    ap.add_argument("--tuning", default=None,
+                    help="threads,layout,chunk,launch[,rows per thread] instead of the autotuner")
     ap.add_argument("--z", type=int, nargs="*", default=None, help="only these z values")
     ap.add_argument("--rates", type=int, nargs="*", default=None, help="only these rates")
     args = ap.parse_args()
@@ -104,29 +105,35 @@ def main():
     if args.sweep:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         for threads in (96, 192):
-            for layout in (wl.MIXED_MSG_REGISTERS, wl.MIXED_MSG_SHARED):
-                for chunk in (8, 16, 32, 64):
-                    for launch in (wl.MIXED_CONCURRENT, wl.MIXED_SERIAL):
-                        mixed.set_tuning(threads, layout, chunk, launch)
-                        mixed.decode_device(variants, offsets, llr, hard, None, status, stream=stream)
-                        e0.record(stream)
-                        for _ in range(3):
+            for rows in (1, 2):
+                for layout in (wl.MIXED_MSG_REGISTERS, wl.MIXED_MSG_SHARED):
+                    for chunk in (8, 16, 32, 64):
+                        for launch in (wl.MIXED_CONCURRENT, wl.MIXED_SERIAL):
+                            mixed.set_tuning(threads, layout, chunk, launch)
+                            mixed.set_rows_per_thread(rows)
                             mixed.decode_device(variants, offsets, llr, hard, None, status, stream=stream)
-                        e1.record(stream)
-                        torch.cuda.synchronize()
-                        mixed.synchronize()
-                        ms = e0.elapsed_time(e1) / 3
-                        table.append({"threads": threads, "messages": ["registers", "shared"][layout], "chunk": chunk,
-                                      "launch": ["concurrent", "serial"][launch], "ms": ms})
-                        print(f"sweep: {threads:3d} threads, messages in {table[-1]['messages']:9s}, chunk {chunk:2d}, "
-                              f"{table[-1]['launch']:10s}: {ms:7.3f} ms")
+                            e0.record(stream)
+                            for _ in range(3):
+                                mixed.decode_device(variants, offsets, llr, hard, None, status, stream=stream)
+                            e1.record(stream)
+                            torch.cuda.synchronize()
+                            mixed.synchronize()
+                            ms = e0.elapsed_time(e1) / 3
+                            table.append({"threads": threads, "rows_per_thread": rows,
+                                          "messages": ["registers", "shared"][layout], "chunk": chunk,
+                                          "launch": ["concurrent", "serial"][launch], "ms": ms})
+                            print(f"sweep: {threads:3d} threads, {rows} row{'s' if rows > 1 else ' '} per thread, "
+                                  f"messages in {table[-1]['messages']:9s}, chunk {chunk:2d}, "
+                                  f"{table[-1]['launch']:10s}: {ms:7.3f} ms")
     if args.tuning:
-        t, l, c, p = (int(x) for x in args.tuning.split(","))
-        mixed.set_tuning(t, l, c, p)
+        vals = [int(x) for x in args.tuning.split(",")]
+        mixed.set_tuning(*vals[:4])
+        mixed.set_rows_per_thread(vals[4] if len(vals) > 4 else 1)
         best = None
     else:
         best = mixed.autotune(variants, offsets, llr, hard, repeats=3)
     threads, layout, chunk, launch = mixed.tuning()
+    rows = mixed.rows_per_thread()
     for _ in range(3):
         mixed.decode_device(variants, offsets, llr, hard, None, status, stream=stream)
     torch.cuda.synchronize()
@@ -156,7 +163,8 @@ def main():
     res = {"workload": f"mixed batch: code uniform over {len(codes)} (rate, z), Eb/N0 U[1, 4] dB, cap 10",
                       "frames": args.frames, "info_bits_per_batch": info_bits,
                       "mixed": {"ms": ms_mixed, "info_gbps": info_bits / (ms_mixed * 1e-3) / 1e9,
-                                "threads": threads, "chunk": chunk, "messages": ["registers", "shared"][layout],
+                                "threads": threads, "rows_per_thread": rows, "chunk": chunk,
+                                "messages": ["registers", "shared"][layout],
                                 "launch": ["concurrent", "serial"][launch], "autotune_best_ms": best},
                       "per_code_launches": {"ms": ms_split, "info_gbps": info_bits / (ms_split * 1e-3) / 1e9,
                                             "launches": len(groups)},
