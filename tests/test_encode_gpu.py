@@ -21,6 +21,7 @@ def test_encoder_golden_device_batch(wl, cuda, golden_encode):
         cw = cw.cpu().numpy()
         assert [inputs.digest(cw[f]) for f in range(c["frames"])] == c["digests"], (c["rate"], c["z"])
         assert inputs.digest(enc.encode(u[1])) == c["digests"][1]
+        assert inputs.digest(enc.encode(u[0])) == c["digests"][0]   # non-0/1 bytes through the single-frame path
 
 
 def test_encoder_large_batch_against_oracle(wl, cuda, oracle):

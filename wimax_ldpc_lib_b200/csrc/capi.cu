@@ -104,6 +104,10 @@ struct wldpc_encoder {
     CodeDesc code;
     cudaStream_t stream = nullptr;
     DevBuf info, cw;
+    /* one frame per call: a device block [info k | codeword n] and its pinned
+     * host image, so a call is one copy each way through pinned memory */
+    DevBuf one;
+    unsigned char* one_host = nullptr;
 };
 
 struct wldpc_ber_runner {
@@ -522,6 +526,7 @@ int wldpc_encoder_destroy(wldpc_encoder* e)
         cudaStreamSynchronize(e->stream);
         cudaStreamDestroy(e->stream);
     }
+    if (e->one_host) cudaFreeHost(e->one_host);
     delete e;
     return WLDPC_OK;
 }
@@ -551,12 +556,28 @@ int wldpc_encode_batch_device(wldpc_encoder* e, const uint8_t* info, uint8_t* co
 int wldpc_encoder_encode(wldpc_encoder* e, const uint8_t* infoword, uint8_t* codeword)
 {
     if (!e || !infoword || !codeword) return WLDPC_ERR_ARG;
+    const size_t k = (size_t)e->code.k, n = (size_t)e->code.n;   /* k and n are multiples of 4 */
     int rc;
-    if ((rc = e->info.reserve((size_t)e->code.k)) || (rc = e->cw.reserve((size_t)e->code.n))) return rc;
-    CU(cudaMemcpyAsync(e->info.p, infoword, (size_t)e->code.k, cudaMemcpyHostToDevice, e->stream));
-    CU(launch_encode_bytes(e->code, (const uint8_t*)e->info.p, (uint8_t*)e->cw.p, 1, e->stream));
-    CU(cudaMemcpyAsync(codeword, e->cw.p, (size_t)e->code.n, cudaMemcpyDeviceToHost, e->stream));
+    if ((rc = e->one.reserve(k + n))) return rc;
+    if (!e->one_host) {
+        void* h = nullptr;
+        if (cudaHostAlloc(&h, k + n, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return WLDPC_ERR_CUDA;
+        }
+        e->one_host = (unsigned char*)h;
+    }
+    unsigned char* dev = (unsigned char*)e->one.p;
+    memcpy(e->one_host, infoword, k);
+    CU(cudaMemcpyAsync(dev, e->one_host, k, cudaMemcpyHostToDevice, e->stream));
+    if (launch_encode_bytes(e->code, dev, dev + k, 1, e->stream) != cudaSuccess ||
+        cudaMemcpyAsync(e->one_host + k, dev + k, n, cudaMemcpyDeviceToHost, e->stream) != cudaSuccess) {
+        cudaStreamSynchronize(e->stream);
+        cudaGetLastError();
+        return WLDPC_ERR_CUDA;
+    }
     CU(cudaStreamSynchronize(e->stream));
+    memcpy(codeword, e->one_host + k, n);
     return WLDPC_OK;
 }
 
