@@ -29,7 +29,8 @@ and is no worse than the plain decoder's, else the plain one's.
   config1    rate 5/6 z=96, 262144 frames at 4 dB, the three decoders
   config2    131072 frames mixed over all 114 codes, one graph launch
   encoder    the dual-diagonal encoder on the headline batch
-  single_frame  decode(float*) one frame per call, next to one reference core
+  single_frame  decode(float*) and BER_runner::run_iteration, one frame per
+             call, next to the reference on one core
   waterfall  rate 1/2 z=96 BER/FER sweep (0.1 dB steps, >= 200 bit errors per
              point) with the plain and the fp32 learned decoder: Eb/N0 at BER 1e-5
 
@@ -602,6 +603,30 @@ def run_ours(args):
             dt = time.perf_counter() - t
             sf["reference_one_core"] = {"frames_per_s": src1.shape[0] / dt, "latency_us": 1e6 * dt / src1.shape[0],
                                         "info_gbps": src1.shape[0] * k / dt / 1e9}
+        # BER_runner::run_iteration, one frame per call (LFSR bits, encode,
+        # BPSK + mt19937 noise on the host, decode, error count), both sides
+        n_ber = 256
+        ber = wl.BERRunner(RATE, Z, 1, MAX_ITER)
+        for _ in range(8):
+            ber.run_iteration(EBNO_DB)
+        t = time.perf_counter()
+        for _ in range(n_ber):
+            ber.run_iteration(EBNO_DB)
+        dt = time.perf_counter() - t
+        ber.close()
+        sf["ber_runner"] = {"api": "wldpc_ber_runner_run_iteration", "frames": n_ber, "frames_per_s": n_ber / dt,
+                            "latency_us": 1e6 * dt / n_ber}
+        if reference_available():
+            L = ref.lib
+            h = L.ref_ber_create(RATE, Z, 1, MAX_ITER)
+            for _ in range(8):
+                L.ref_ber_run_iteration(h, EBNO_DB)
+            t = time.perf_counter()
+            for _ in range(n_ber):
+                L.ref_ber_run_iteration(h, EBNO_DB)
+            dt = time.perf_counter() - t
+            L.ref_ber_destroy(h)
+            sf["ber_runner"]["reference_one_thread"] = {"frames_per_s": n_ber / dt, "latency_us": 1e6 * dt / n_ber}
         extra["single_frame"] = sf
 
     # config 4 for the headline code: the full-device waterfall of the plain and
