@@ -134,7 +134,7 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
     constexpr int MB = S::MB, N = S::N, G = S::G;
     extern __shared__ __align__(128) float smem_lms[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ unsigned s_fail[2];
+    __shared__ unsigned s_fail[2], s_last[2];
 
     const int tid = threadIdx.x;
     const int g = G == 1 ? 0 : tid / Z;
@@ -151,6 +151,8 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         fence_mbar_init();
         s_fail[0] = 0;
         s_fail[1] = 0;
+        s_last[0] = 0;
+        s_last[1] = 0;
         const uint32_t bytes = (uint32_t)(nf * N * 4);
         mbar_arrive_expect_tx(&bar, bytes);
         bulk_g2s(smem_lms, a.llr + f0 * N, bytes, &bar);
@@ -165,9 +167,10 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         return;
     }
 
-    auto rows_fail = [&]() -> unsigned {
+    /* syndrome of the thread's rows in layers 0 .. LAYERS-1: 1 if any fails */
+    auto rows_fail = [&](auto LAYERS) -> unsigned {
         unsigned fail = 0;
-        static_for<MB>([&](auto I) {
+        static_for<decltype(LAYERS)::value>([&](auto I) {
             constexpr int d = layer_degree(R, I);
             bool odd = (d & 1) != 0;   /* parity of the hard bits: d minus the negatives */
             static_for<d>([&](auto E_) {
@@ -177,13 +180,14 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         });
         return fail;
     };
-    auto frame_fail = [&](unsigned fail, int slot) -> unsigned {
+    /* per-frame OR over the CTA (bit g: frame g); one barrier */
+    auto frame_fail = [&](unsigned fail, unsigned* slot) -> unsigned {
         if constexpr (G == 1) {
             return __syncthreads_or((int)fail) ? 1u : 0u;
         } else {
-            if (fail) atomicOr(&s_fail[slot], 1u << g);
+            if (fail) atomicOr(slot, 1u << g);
             __syncthreads();
-            return s_fail[slot];
+            return *slot;
         }
     };
 
@@ -194,17 +198,25 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
     for (int q = 0; q < S::NBLK; q++) Mr[q] = 0.0f;
 
     const bool live = g < nf;
-    unsigned fmask = frame_fail(live ? rows_fail() : 0u, 0);
+    unsigned fmask = frame_fail(live ? rows_fail(std::integral_constant<int, MB>{}) : 0u, &s_fail[0]);
     bool active = live && ((fmask >> g) & 1u);
     int iters = 0;
 
     for (int t = 0; t < a.iters && fmask != 0u; ++t) {
+        const int slot = (t + 1) & 1;   /* read last two iterations ago, before many barriers */
         if constexpr (G > 1) {
-            if (tid == 0) s_fail[(t + 1) & 1] = 0;
+            if (tid == 0) {
+                s_fail[slot] = 0;
+                s_last[slot] = 0;
+            }
         }
+        /* parity of the last layer's row from the posteriors it writes: no
+         * later layer changes them in this iteration, so they are final */
+        bool last_odd = false;
         static_for<MB>([&](auto I) {
             constexpr int d = layer_degree(R, I);
             constexpr int b0 = block_index(R, I, 0);
+            constexpr bool LAST = decltype(I)::value == MB - 1;
             if (active) {
                 float L[d];
                 uint32_t sgn = 0;
@@ -230,12 +242,22 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
                     const float mag = fmaxf(__fmaf_rn(ab.x, mu, -ab.y), 0.0f);
                     const float msg = __fmul_rn(mag, __uint_as_float((__float_as_uint(l) & 0x80000000u) ^ fbo));
                     Mr[b0 + e] = msg;
-                    *lms_edge<R, Z, I, e>(P, Pr, Prz, r) = __fadd_rn(l, msg);
+                    const float pn = __fadd_rn(l, msg);
+                    *lms_edge<R, Z, I, e>(P, Pr, Prz, r) = pn;
+                    if constexpr (LAST) last_odd = last_odd != (pn < 0.0f);
                 });
+                if constexpr (LAST) last_odd = last_odd != ((d & 1) != 0);
             }
-            __syncthreads();
+            if constexpr (!LAST) __syncthreads();
         });
-        fmask = frame_fail(live && active ? rows_fail() : 0u, (t + 1) & 1);
+        /* stopping rule (zero syndrome over every row): a frame with a failing
+         * row in the last layer fails; the other active frames check the
+         * remaining layers. The first vote is the last layer's barrier. */
+        const unsigned lmask = frame_fail(active && last_odd ? 1u : 0u, &s_last[slot]);
+        unsigned full = 0;
+        if (fmask & ~lmask)
+            full = frame_fail(active && !((lmask >> g) & 1u) ? rows_fail(std::integral_constant<int, MB - 1>{}) : 0u, &s_fail[slot]);
+        fmask = lmask | full;
         if (active) {
             iters = t + 1;
             active = (fmask >> g) & 1u;

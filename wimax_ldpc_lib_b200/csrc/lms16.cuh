@@ -206,7 +206,7 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
     constexpr int STEPS = GP * V4 / TH;       /* staging / output groups per thread (6) */
     static_assert(GP * V4 % TH == 0, "staging must divide evenly");
     __shared__ __align__(16) uint32_t sP[GP * N];
-    __shared__ unsigned s_fail[2];
+    __shared__ unsigned s_fail[2], s_last[2];
 
     const int tid = threadIdx.x;
     const int g = GP == 1 ? 0 : tid / Z;
@@ -227,6 +227,8 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
     if (tid == 0) {
         s_fail[0] = 0;
         s_fail[1] = 0;
+        s_last[0] = 0;
+        s_last[1] = 0;
     }
     /* staging: word v of pair q holds variable v of frames 2q (low lane) and
      * 2q+1 (high lane); all loads are issued before the conversions */
@@ -255,10 +257,11 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
     }
     __syncthreads();
 
-    /* sign bit of each lane: set where some row of that frame fails */
-    auto rows_fail = [&]() -> uint32_t {
+    /* sign bit of each lane: set where some row of that frame fails, over
+     * layers 0 .. LAYERS-1 */
+    auto rows_fail = [&](auto LAYERS) -> uint32_t {
         uint32_t acc = 0;
-        static_for<MB>([&](auto I) {
+        static_for<decltype(LAYERS)::value>([&](auto I) {
             constexpr int d = layer_degree(R, I);
             uint32_t x = (d & 1) ? kH2Sign : 0u;   /* parity of the hard bits: d minus the negatives */
             static_for<d>([&](auto E_) { x ^= *at(I, E_); });
@@ -270,12 +273,12 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
      * of 32 the last warp is partial and its reduction covers only its lanes. */
     constexpr unsigned kTailLanes = TH % 32;
     const unsigned wmask = (kTailLanes == 0 || tid < TH - (int)kTailLanes) ? 0xffffffffu : (1u << kTailLanes) - 1u;
-    auto frame_fail = [&](uint32_t acc, int slot) -> unsigned {
+    auto frame_fail = [&](uint32_t acc, unsigned* slot) -> unsigned {
         unsigned bits = (((acc >> 15) & 1u) | ((acc >> 30) & 2u)) << (2 * g);
         bits = __reduce_or_sync(wmask, bits);
-        if ((tid & 31) == 0 && bits) atomicOr(&s_fail[slot], bits);
+        if ((tid & 31) == 0 && bits) atomicOr(slot, bits);
         __syncthreads();
-        return s_fail[slot];
+        return *slot;
     };
 
     uint32_t Mr[S::NBLK];
@@ -283,17 +286,25 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
     for (int q = 0; q < S::NBLK; q++) Mr[q] = 0u;
 
     const unsigned live = (2 * g < nf ? 1u : 0u) | (2 * g + 1 < nf ? 2u : 0u);
-    unsigned fmask = frame_fail(live ? rows_fail() & h2_lanes(live) : 0u, 0);
+    unsigned fmask = frame_fail(live ? rows_fail(std::integral_constant<int, MB>{}) & h2_lanes(live) : 0u, &s_fail[0]);
     unsigned act = (fmask >> (2 * g)) & 3u;   /* lanes of this pair still decoding */
     int it0 = 0, it1 = 0;
 
     for (int t = 0; t < a.iters && fmask != 0u; ++t) {
-        if (tid == 0) s_fail[(t + 1) & 1] = 0;
+        const int slot = (t + 1) & 1;   /* last read two iterations ago, before many barriers */
+        if (tid == 0) {
+            s_fail[slot] = 0;
+            s_last[slot] = 0;
+        }
         const uint32_t am = h2_lanes(act);     /* lanes still decoding; frozen lanes get mu = 0 */
         const uint2* wab = a.wab[t < a.wrows ? t : a.wrows - 1];
+        /* parity of the last layer's row from the posteriors it writes (no
+         * later layer changes them in this iteration): sign bit per lane */
+        uint32_t last_par = 0;
         static_for<MB>([&](auto I) {
             constexpr int d = layer_degree(R, I);
             constexpr int b0 = block_index(R, I, 0);
+            constexpr bool LAST = decltype(I)::value == MB - 1;
             if (act) {
                 uint32_t L[d], A[d];
                 uint32_t sgn = 0;
@@ -319,11 +330,23 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
                     Mr[b0 + e] = msg;
                     const uint32_t pn = h2_add(L[e], msg);
                     *at(I, E_) = pn;
+                    if constexpr (LAST) last_par ^= pn;
                 });
+                if constexpr (LAST) last_par = (last_par ^ ((d & 1) ? kH2Sign : 0u)) & kH2Sign;
             }
-            __syncthreads();
+            if constexpr (!LAST) __syncthreads();
         });
-        fmask = frame_fail(act ? rows_fail() & h2_lanes(act) : 0u, (t + 1) & 1);
+        /* stopping rule: a lane with a failing row in the last layer fails;
+         * the other active lanes check the remaining layers. The first vote
+         * is the last layer's barrier. */
+        const unsigned lmask = frame_fail(act ? last_par & h2_lanes(act) : 0u, &s_last[slot]);
+        unsigned full = 0;
+        if (fmask & ~lmask) {
+            const unsigned chk = act & ~(lmask >> (2 * g)) & 3u;
+            full = frame_fail(chk ? rows_fail(std::integral_constant<int, MB - 1>{}) & h2_lanes(chk) : 0u,
+                              &s_fail[slot]);
+        }
+        fmask = lmask | full;
         if (act & 1u) it0 = t + 1;
         if (act & 2u) it1 = t + 1;
         const unsigned nact = (fmask >> (2 * g)) & 3u;

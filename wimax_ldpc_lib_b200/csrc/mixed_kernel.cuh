@@ -172,8 +172,10 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
             if (tid == 0) S.phase ^= S.fresh;   /* every refilled slot's barrier completed one phase */
         }
 
-        /* 2. syndrome of the slots loaded or iterated since their last check */
-        if (in_slot && frame >= 0 && need_check) {
+        /* 2. syndrome of the slots loaded or iterated since their last check;
+         * a slot whose last layer already failed in step 5 (bit g of S.fail,
+         * set before that step's last barrier) needs no full check */
+        if (in_slot && frame >= 0 && need_check && !((*(volatile unsigned*)&S.fail >> g) & 1u)) {
             unsigned fail = 0;
 #pragma unroll
             for (int k = 0; k < RPT; k++)
@@ -215,7 +217,7 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
             all_empty &= S.frame[q] < 0;
         }
         const bool more = S.next < item.count;
-        if (tid == 0) S.fail = 0;   /* read only in step 3, before the barrier above */
+        if (tid == 0) S.fail = 0;   /* read in steps 2 and 3, before the barrier above; set again from step 5 on */
         if (all_empty && !more) break;
         refill = any_empty && more;
         if (refill) {
@@ -223,12 +225,17 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
             continue;
         }
 
-        /* 5. one iteration of every occupied slot (all of them failed their check) */
+        /* 5. one iteration of every occupied slot (all of them failed their
+         * check). The last layer's rows also check their parity on the
+         * posteriors they write, which no later layer changes in this
+         * iteration: a failing one marks its slot in S.fail. */
         const bool active = in_slot && frame >= 0;
         static_for<MB>([&](auto I) {
             constexpr int i = decltype(I)::value;
             constexpr int d = layer_degree(R, i);
+            constexpr bool LAST = i == MB - 1;
             if (active) {
+                bool last_fail = false;
                 /* the layer's rows (independent chains), each with its edge
                  * addresses loaded once for both passes */
 #pragma unroll
@@ -238,16 +245,21 @@ __device__ __forceinline__ bool mixed_item(const MixedArgs& a, const MixedItem i
                         ad[decltype(E)::value] = addr(k, block_index(R, i, decltype(E)::value));
                     });
                     auto at = [&](auto E) { return P + ad[decltype(E)::value]; };
+                    bool odd = false;
                     if constexpr (LAYOUT == kMsgRegisters) {
-                        tdmp_layer<R, i, kNms>(at, rM1[k][i], rM2[k][i], rNEG[k][i]);
+                        tdmp_layer<R, i, kNms, LAST>(at, rM1[k][i], rM2[k][i], rNEG[k][i], &odd);
                     } else {
                         float a1 = sM1(k, i), a2 = sM2(k, i);
                         uint32_t ng = sNEG(k, i);
-                        tdmp_layer<R, i, kNms>(at, a1, a2, ng);
+                        tdmp_layer<R, i, kNms, LAST>(at, a1, a2, ng, &odd);
                         sM1(k, i) = a1;
                         sM2(k, i) = a2;
                         sNEG(k, i) = ng;
                     }
+                    last_fail |= odd;
+                }
+                if constexpr (LAST) {
+                    if (last_fail) atomicOr(&S.fail, 1u << g);
                 }
             }
             __syncthreads();

@@ -145,9 +145,11 @@ __device__ __forceinline__ float canon(float x) { return __fadd_rn(x, 0.0f); }
  * messages and posteriors in the mode's arithmetic) and the new compressed
  * messages M1, M2 (rounded magnitudes) and NEG (sign bit d-1-e of edge e |
  * argmin edge << 27). at(e) gives the posterior of edge e of this layer for
- * this row. Used by the specialised decoder and by the mixed-code decoder. */
-template <int R, int I, int MODE, typename At>
-__device__ __forceinline__ void tdmp_layer(At&& at, float& M1, float& M2, uint32_t& NEG)
+ * this row. Used by the specialised decoder and by the mixed-code decoder.
+ * With PAR, *odd is set to whether the row fails the parity check on the
+ * posteriors this layer writes (hard bit x >= 0). */
+template <int R, int I, int MODE, bool PAR = false, typename At>
+__device__ __forceinline__ void tdmp_layer(At&& at, float& M1, float& M2, uint32_t& NEG, bool* odd = nullptr)
 {
     constexpr int d = layer_degree(R, I);
     float L[d];
@@ -177,6 +179,7 @@ __device__ __forceinline__ void tdmp_layer(At&& at, float& M1, float& M2, uint32
     const uint32_t flip = (uint32_t)((d & 1) ^ (__popc(sgn) & 1));
     const uint32_t dmask = (d >= 32) ? 0xffffffffu : ((1u << d) - 1u);
     int nIdx = 0;
+    bool par = false;   /* parity of the negative posteriors written (PAR) */
     if constexpr (MODE == kMs) {
         const uint32_t fb = flip << 31;
         static_for<d>([&](auto E) {
@@ -187,7 +190,9 @@ __device__ __forceinline__ void tdmp_layer(At&& at, float& M1, float& M2, uint32
             nIdx = is_min ? e : nIdx;
             const uint32_t sb = (LC[e] & 0x80000000u) ^ fb;
             const float t = __uint_as_float(__float_as_uint(mu) | sb);
-            *at(E) = __fadd_rn(l, t);
+            const float pn = __fadd_rn(l, t);
+            *at(E) = pn;
+            if constexpr (PAR) par = par != (pn < 0.0f);
         });
         M1 = m1;
         M2 = m2;
@@ -214,21 +219,25 @@ __device__ __forceinline__ void tdmp_layer(At&& at, float& M1, float& M2, uint32
             const int lo = is_min ? l2 : l1;
             hi ^= (int)(LC[e] & 0x80000000u);
             const double t = __hiloint2double(hi, lo);
-            *at(E) = __double2float_rn(__dadd_rn((double)l, t));
+            const float pn = __double2float_rn(__dadd_rn((double)l, t));
+            *at(E) = pn;
+            if constexpr (PAR) par = par != (pn < 0.0f);
         });
         M1 = __double2float_rn(D1);
         M2 = __double2float_rn(D2);
     }
     NEG = ((sgn ^ (flip ? dmask : 0u)) & dmask) | ((uint32_t)nIdx << 27);
+    if constexpr (PAR) *odd = par != ((d & 1) != 0);
 }
 
 /* The same layer with one message per edge kept as a float in a register
  * (Mr, indexed by block), normalized min-sum only: pass 1 reads the old
  * message directly instead of rebuilding it from M1 / M2 / NEG. The stored
  * values are identical to the compressed form's (+-float(D1) or
- * +-float(D2)): where several edges tie at the minimum, D1 == D2. */
-template <int R, int I, typename At, int NB>
-__device__ __forceinline__ void tdmp_layer_edges(At&& at, float (&Mr)[NB])
+ * +-float(D2)): where several edges tie at the minimum, D1 == D2. PAR and
+ * odd as in tdmp_layer. */
+template <int R, int I, bool PAR = false, typename At, int NB>
+__device__ __forceinline__ void tdmp_layer_edges(At&& at, float (&Mr)[NB], bool* odd = nullptr)
 {
     constexpr int d = layer_degree(R, I);
     constexpr int b0 = block_index(R, I, 0);
@@ -253,6 +262,7 @@ __device__ __forceinline__ void tdmp_layer_edges(At&& at, float (&Mr)[NB])
     const uint32_t f1 = __float_as_uint(__double2float_rn(D1)) | fb, f2 = __float_as_uint(__double2float_rn(D2)) | fb;
     const int h1 = __double2hiint(D1) ^ (int)fb, l1 = __double2loint(D1);
     const int h2 = __double2hiint(D2) ^ (int)fb, l2 = __double2loint(D2);
+    bool par = false;
     static_for<d>([&](auto E) {
         constexpr int e = decltype(E)::value;
         const float l = L[e];
@@ -261,9 +271,12 @@ __device__ __forceinline__ void tdmp_layer_edges(At&& at, float (&Mr)[NB])
         int hi = is_min ? h2 : h1;
         const int lo = is_min ? l2 : l1;
         hi ^= (int)sb;
-        *at(E) = __double2float_rn(__dadd_rn((double)l, __hiloint2double(hi, lo)));
+        const float pn = __double2float_rn(__dadd_rn((double)l, __hiloint2double(hi, lo)));
+        *at(E) = pn;
+        if constexpr (PAR) par = par != (pn < 0.0f);
         Mr[b0 + e] = __uint_as_float((is_min ? f2 : f1) ^ sb);
     });
+    if constexpr (PAR) *odd = par != ((d & 1) != 0);
 }
 
 /* Which message layout the specialised normalized min-sum decoder uses: one
@@ -280,14 +293,15 @@ constexpr bool tdmp_edge_messages(int rate, int z, int mode)
            ((kEdgeMsgZ[rate] >> ((z - kZMin) / kZStep)) & 1u) != 0;
 }
 
-/* Syndrome of the thread's rows over all layers: 1 if any row fails. The
+/* Syndrome of the thread's rows in layers 0 .. LAYERS-1 (default: all): 1 if
+ * any row fails. The
  * hard decision is x >= 0 (-0.0 is bit 1); a row of degree d fails when d
  * minus its number of negative posteriors is odd. at(I, E) as in tdmp_layer. */
-template <int R, typename At>
+template <int R, int LAYERS = kMb[R], typename At>
 __device__ __forceinline__ unsigned tdmp_rows_fail(At&& at)
 {
     unsigned fail = 0;
-    static_for<kMb[R]>([&](auto I) {
+    static_for<LAYERS>([&](auto I) {
         constexpr int d = layer_degree(R, I);
         bool odd = (d & 1) != 0;
         static_for<d>([&](auto E) { odd = odd != (*at(I, E) < 0.0f); });
@@ -307,7 +321,7 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
     const int nthreads = G * Z;
     extern __shared__ __align__(128) float smem_post[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ unsigned s_fail[2];
+    __shared__ unsigned s_fail[2], s_last[2];
 
     const int tid = threadIdx.x;
     const int g = G == 1 ? 0 : tid / Z;
@@ -324,6 +338,8 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
         fence_mbar_init();
         s_fail[0] = 0;
         s_fail[1] = 0;
+        s_last[0] = 0;
+        s_last[1] = 0;
         const uint32_t bytes = (uint32_t)(nf * N * 4);
         mbar_arrive_expect_tx(&bar, bytes);
         bulk_g2s(smem_post, a.llr + f0 * N, bytes, &bar);
@@ -338,30 +354,27 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
         return;
     }
 
-    /* syndrome of the current posterior for this thread's rows: 1 if any fails */
-    auto rows_fail = [&]() -> unsigned {
-        return tdmp_rows_fail<R>([&](auto I, auto E) {
+    /* syndrome of the current posterior for this thread's rows in layers
+     * 0 .. LAYERS-1: 1 if any fails */
+    auto rows_fail = [&](auto LAYERS) -> unsigned {
+        return tdmp_rows_fail<R, decltype(LAYERS)::value>([&](auto I, auto E) {
             return post_ptr<R, ZT, decltype(I)::value, decltype(E)::value>(P, Pr, Prz, r, a);
         });
     };
-    /* per-frame OR over the CTA; returns this frame's flag and whether any
-     * live frame is still failing */
-    auto frame_fail = [&](unsigned fail, int slot, bool& any) -> bool {
+    /* per-frame OR over the CTA (bit g: frame g); one barrier */
+    auto frame_fail = [&](unsigned fail, unsigned* slot) -> unsigned {
         if constexpr (G == 1) {
-            any = __syncthreads_or((int)fail) != 0;
-            return any;
+            return __syncthreads_or((int)fail) ? 1u : 0u;
         } else {
-            if (fail) atomicOr(&s_fail[slot], 1u << g);
+            if (fail) atomicOr(slot, 1u << g);
             __syncthreads();
-            const unsigned m = s_fail[slot];
-            any = m != 0;
-            return (m >> g) & 1u;
+            return *slot;
         }
     };
 
     const bool live = g < nf;
-    bool any_fail;
-    bool active = frame_fail(live ? rows_fail() : 0u, 0, any_fail);
+    unsigned fmask = frame_fail(live ? rows_fail(std::integral_constant<int, MB>{}) : 0u, &s_fail[0]);
+    bool active = live && ((fmask >> g) & 1u);
     int iters = 0;
 
     /* compressed messages per layer: magnitudes and NEG = sign bits (bit
@@ -375,24 +388,41 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
 #pragma unroll
     for (int q = 0; q < (EDGE_MSGS ? num_blocks(R) : 1); q++) Mr[q] = 0.0f;
 
-    for (int it = 1; it <= a.max_iter && any_fail; ++it) {
+    for (int it = 1; it <= a.max_iter && fmask != 0u; ++it) {
+        const int slot = it & 1;   /* last read two iterations ago, before many barriers */
         if constexpr (G > 1) {
-            if (tid == 0) s_fail[it & 1] = 0;   /* slot it&1 was last read before the previous barrier */
+            if (tid == 0) {
+                s_fail[slot] = 0;
+                s_last[slot] = 0;
+            }
         }
+        /* parity of the last layer's row from the posteriors it writes: no
+         * later layer changes them in this iteration, so they are final */
+        bool last_odd = false;
         static_for<MB>([&](auto I) {
+            constexpr bool LAST = decltype(I)::value == MB - 1;
             if (active) {
                 auto at = [&](auto E) { return post_ptr<R, ZT, decltype(I)::value, decltype(E)::value>(P, Pr, Prz, r, a); };
                 if constexpr (EDGE_MSGS)
-                    tdmp_layer_edges<R, decltype(I)::value>(at, Mr);
+                    tdmp_layer_edges<R, decltype(I)::value, LAST>(at, Mr, &last_odd);
                 else
-                    tdmp_layer<R, decltype(I)::value, MODE>(at, M1[I], M2[I], NEG[I]);
+                    tdmp_layer<R, decltype(I)::value, MODE, LAST>(at, M1[I], M2[I], NEG[I], &last_odd);
             }
-            __syncthreads();
+            if constexpr (!LAST) __syncthreads();
         });
-        const bool f = frame_fail(live && active ? rows_fail() : 0u, it & 1, any_fail);
+        /* stopping rule (zero syndrome over every row, reference
+         * lib/ldpc_decoder.cc:242-251): a frame with a failing row in the last
+         * layer fails; the other active frames check the remaining layers. The
+         * first vote is the last layer's barrier. */
+        const unsigned lmask = frame_fail(active && last_odd ? 1u : 0u, &s_last[slot]);
+        unsigned full = 0;
+        if (fmask & ~lmask)
+            full = frame_fail(active && !((lmask >> g) & 1u) ? rows_fail(std::integral_constant<int, MB - 1>{}) : 0u,
+                              &s_fail[slot]);
+        fmask = lmask | full;
         if (active) {
             iters = it;
-            active = f;
+            active = (fmask >> g) & 1u;
         }
     }
 
