@@ -167,14 +167,15 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         return;
     }
 
-    /* syndrome of the thread's rows in layers 0 .. LAYERS-1: 1 if any fails */
-    auto rows_fail = [&](auto LAYERS) -> unsigned {
+    /* syndrome of the thread's rows in layers FIRST .. END-1: 1 if any fails */
+    auto rows_fail = [&](auto FIRST, auto END) -> unsigned {
         unsigned fail = 0;
-        static_for<decltype(LAYERS)::value>([&](auto I) {
-            constexpr int d = layer_degree(R, I);
+        static_for<decltype(END)::value - decltype(FIRST)::value>([&](auto I_) {
+            using I = std::integral_constant<int, decltype(FIRST)::value + decltype(I_)::value>;
+            constexpr int d = layer_degree(R, I::value);
             bool odd = (d & 1) != 0;   /* parity of the hard bits: d minus the negatives */
             static_for<d>([&](auto E_) {
-                odd = odd != (*lms_edge<R, Z, I, E_>(P, Pr, Prz, r) < 0.0f);
+                odd = odd != (*lms_edge<R, Z, I::value, E_>(P, Pr, Prz, r) < 0.0f);
             });
             fail |= odd ? 1u : 0u;
         });
@@ -197,8 +198,17 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
 #pragma unroll
     for (int q = 0; q < S::NBLK; q++) Mr[q] = 0.0f;
 
+    /* initial syndrome (reference lib/ldpc_decoder.cc:127-139): layer 0's
+     * rows first; only frames that pass there check the other layers */
+    using L0 = std::integral_constant<int, 0>;
+    using L1 = std::integral_constant<int, 1>;
+    using LM = std::integral_constant<int, MB - 1>;
+    using LE = std::integral_constant<int, MB>;
     const bool live = g < nf;
-    unsigned fmask = frame_fail(live ? rows_fail(std::integral_constant<int, MB>{}) : 0u, &s_fail[0]);
+    const unsigned lives = (1u << nf) - 1u;
+    unsigned fmask = frame_fail(live ? rows_fail(L0{}, L1{}) : 0u, &s_last[0]);
+    if (lives & ~fmask)
+        fmask |= frame_fail(live && !((fmask >> g) & 1u) ? rows_fail(L1{}, LE{}) : 0u, &s_fail[0]);
     bool active = live && ((fmask >> g) & 1u);
     int iters = 0;
 
@@ -256,7 +266,7 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         const unsigned lmask = frame_fail(active && last_odd ? 1u : 0u, &s_last[slot]);
         unsigned full = 0;
         if (fmask & ~lmask)
-            full = frame_fail(active && !((lmask >> g) & 1u) ? rows_fail(std::integral_constant<int, MB - 1>{}) : 0u, &s_fail[slot]);
+            full = frame_fail(active && !((lmask >> g) & 1u) ? rows_fail(L0{}, LM{}) : 0u, &s_fail[slot]);
         fmask = lmask | full;
         if (active) {
             iters = t + 1;

@@ -258,13 +258,14 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
     __syncthreads();
 
     /* sign bit of each lane: set where some row of that frame fails, over
-     * layers 0 .. LAYERS-1 */
-    auto rows_fail = [&](auto LAYERS) -> uint32_t {
+     * layers FIRST .. END-1 */
+    auto rows_fail = [&](auto FIRST, auto END) -> uint32_t {
         uint32_t acc = 0;
-        static_for<decltype(LAYERS)::value>([&](auto I) {
-            constexpr int d = layer_degree(R, I);
+        static_for<decltype(END)::value - decltype(FIRST)::value>([&](auto I_) {
+            using I = std::integral_constant<int, decltype(FIRST)::value + decltype(I_)::value>;
+            constexpr int d = layer_degree(R, I::value);
             uint32_t x = (d & 1) ? kH2Sign : 0u;   /* parity of the hard bits: d minus the negatives */
-            static_for<d>([&](auto E_) { x ^= *at(I, E_); });
+            static_for<d>([&](auto E_) { x ^= *at(I{}, E_); });
             acc |= x;
         });
         return acc & kH2Sign;
@@ -286,7 +287,17 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
     for (int q = 0; q < S::NBLK; q++) Mr[q] = 0u;
 
     const unsigned live = (2 * g < nf ? 1u : 0u) | (2 * g + 1 < nf ? 2u : 0u);
-    unsigned fmask = frame_fail(live ? rows_fail(std::integral_constant<int, MB>{}) & h2_lanes(live) : 0u, &s_fail[0]);
+    /* initial syndrome: layer 0's rows first; only lanes that pass there
+     * check the other layers */
+    using L0 = std::integral_constant<int, 0>;
+    using L1 = std::integral_constant<int, 1>;
+    using LM = std::integral_constant<int, MB - 1>;
+    using LE = std::integral_constant<int, MB>;
+    unsigned fmask = frame_fail(live ? rows_fail(L0{}, L1{}) & h2_lanes(live) : 0u, &s_last[0]);
+    if (((1u << nf) - 1u) & ~fmask) {
+        const unsigned chk = live & ~(fmask >> (2 * g)) & 3u;
+        fmask |= frame_fail(chk ? rows_fail(L1{}, LE{}) & h2_lanes(chk) : 0u, &s_fail[0]);
+    }
     unsigned act = (fmask >> (2 * g)) & 3u;   /* lanes of this pair still decoding */
     int it0 = 0, it1 = 0;
 
@@ -343,7 +354,7 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
         unsigned full = 0;
         if (fmask & ~lmask) {
             const unsigned chk = act & ~(lmask >> (2 * g)) & 3u;
-            full = frame_fail(chk ? rows_fail(std::integral_constant<int, MB - 1>{}) & h2_lanes(chk) : 0u,
+            full = frame_fail(chk ? rows_fail(L0{}, LM{}) & h2_lanes(chk) : 0u,
                               &s_fail[slot]);
         }
         fmask = lmask | full;

@@ -293,18 +293,19 @@ constexpr bool tdmp_edge_messages(int rate, int z, int mode)
            ((kEdgeMsgZ[rate] >> ((z - kZMin) / kZStep)) & 1u) != 0;
 }
 
-/* Syndrome of the thread's rows in layers 0 .. LAYERS-1 (default: all): 1 if
- * any row fails. The
+/* Syndrome of the thread's rows in layers FIRST .. END-1 (default: all): 1
+ * if any row fails. The
  * hard decision is x >= 0 (-0.0 is bit 1); a row of degree d fails when d
  * minus its number of negative posteriors is odd. at(I, E) as in tdmp_layer. */
-template <int R, int LAYERS = kMb[R], typename At>
+template <int R, int FIRST = 0, int END = kMb[R], typename At>
 __device__ __forceinline__ unsigned tdmp_rows_fail(At&& at)
 {
     unsigned fail = 0;
-    static_for<LAYERS>([&](auto I) {
-        constexpr int d = layer_degree(R, I);
+    static_for<END - FIRST>([&](auto I_) {
+        using I = std::integral_constant<int, FIRST + decltype(I_)::value>;
+        constexpr int d = layer_degree(R, I::value);
         bool odd = (d & 1) != 0;
-        static_for<d>([&](auto E) { odd = odd != (*at(I, E) < 0.0f); });
+        static_for<d>([&](auto E) { odd = odd != (*at(I{}, E) < 0.0f); });
         fail |= odd ? 1u : 0u;
     });
     return fail;
@@ -355,9 +356,9 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
     }
 
     /* syndrome of the current posterior for this thread's rows in layers
-     * 0 .. LAYERS-1: 1 if any fails */
-    auto rows_fail = [&](auto LAYERS) -> unsigned {
-        return tdmp_rows_fail<R, decltype(LAYERS)::value>([&](auto I, auto E) {
+     * FIRST .. END-1: 1 if any fails */
+    auto rows_fail = [&](auto FIRST, auto END) -> unsigned {
+        return tdmp_rows_fail<R, decltype(FIRST)::value, decltype(END)::value>([&](auto I, auto E) {
             return post_ptr<R, ZT, decltype(I)::value, decltype(E)::value>(P, Pr, Prz, r, a);
         });
     };
@@ -372,8 +373,17 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
         }
     };
 
+    /* initial syndrome (reference lib/ldpc_decoder.cc:127-139): layer 0's
+     * rows first; only frames that pass there check the other layers */
+    using L0 = std::integral_constant<int, 0>;
+    using L1 = std::integral_constant<int, 1>;
+    using LM = std::integral_constant<int, MB - 1>;
+    using LE = std::integral_constant<int, MB>;
     const bool live = g < nf;
-    unsigned fmask = frame_fail(live ? rows_fail(std::integral_constant<int, MB>{}) : 0u, &s_fail[0]);
+    const unsigned lives = (1u << nf) - 1u;
+    unsigned fmask = frame_fail(live ? rows_fail(L0{}, L1{}) : 0u, &s_last[0]);
+    if (lives & ~fmask)
+        fmask |= frame_fail(live && !((fmask >> g) & 1u) ? rows_fail(L1{}, LE{}) : 0u, &s_fail[0]);
     bool active = live && ((fmask >> g) & 1u);
     int iters = 0;
 
@@ -417,7 +427,7 @@ tdmp_decode_kernel(const __grid_constant__ DecodeArgs a)
         const unsigned lmask = frame_fail(active && last_odd ? 1u : 0u, &s_last[slot]);
         unsigned full = 0;
         if (fmask & ~lmask)
-            full = frame_fail(active && !((lmask >> g) & 1u) ? rows_fail(std::integral_constant<int, MB - 1>{}) : 0u,
+            full = frame_fail(active && !((lmask >> g) & 1u) ? rows_fail(L0{}, LM{}) : 0u,
                               &s_fail[slot]);
         fmask = lmask | full;
         if (active) {
