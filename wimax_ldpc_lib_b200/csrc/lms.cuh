@@ -134,7 +134,7 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
     constexpr int MB = S::MB, N = S::N, G = S::G;
     extern __shared__ __align__(128) float smem_lms[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ unsigned s_fail[2], s_last[2];
+    __shared__ unsigned s_fail[2], s_last[2], s_half[2];
 
     const int tid = threadIdx.x;
     const int g = G == 1 ? 0 : tid / Z;
@@ -153,6 +153,8 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         s_fail[1] = 0;
         s_last[0] = 0;
         s_last[1] = 0;
+        s_half[0] = 0;
+        s_half[1] = 0;
         const uint32_t bytes = (uint32_t)(nf * N * 4);
         mbar_arrive_expect_tx(&bar, bytes);
         bulk_g2s(smem_lms, a.llr + f0 * N, bytes, &bar);
@@ -203,6 +205,7 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
     using L0 = std::integral_constant<int, 0>;
     using L1 = std::integral_constant<int, 1>;
     using LM = std::integral_constant<int, MB - 1>;
+    using LH = std::integral_constant<int, (MB - 1) / 2>;
     using LE = std::integral_constant<int, MB>;
     const bool live = g < nf;
     const unsigned lives = (1u << nf) - 1u;
@@ -218,6 +221,7 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
             if (tid == 0) {
                 s_fail[slot] = 0;
                 s_last[slot] = 0;
+                s_half[slot] = 0;
             }
         }
         /* parity of the last layer's row from the posteriors it writes: no
@@ -262,12 +266,16 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         });
         /* stopping rule (zero syndrome over every row): a frame with a failing
          * row in the last layer fails; the other active frames check the
-         * remaining layers. The first vote is the last layer's barrier. */
+         * remaining layers in two halves, with a vote after each (a frame that
+         * fails in the first half skips the second). The first vote is the last
+         * layer's barrier. */
         const unsigned lmask = frame_fail(active && last_odd ? 1u : 0u, &s_last[slot]);
-        unsigned full = 0;
-        if (fmask & ~lmask)
-            full = frame_fail(active && !((lmask >> g) & 1u) ? rows_fail(L0{}, LM{}) : 0u, &s_fail[slot]);
-        fmask = lmask | full;
+        unsigned fm = lmask;
+        if (fmask & ~fm)
+            fm |= frame_fail(active && !((fm >> g) & 1u) ? rows_fail(L0{}, LH{}) : 0u, &s_fail[slot]);
+        if (fmask & ~fm)
+            fm |= frame_fail(active && !((fm >> g) & 1u) ? rows_fail(LH{}, LM{}) : 0u, &s_half[slot]);
+        fmask = fm;
         if (active) {
             iters = t + 1;
             active = (fmask >> g) & 1u;

@@ -206,7 +206,7 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
     constexpr int STEPS = GP * V4 / TH;       /* staging / output groups per thread (6) */
     static_assert(GP * V4 % TH == 0, "staging must divide evenly");
     __shared__ __align__(16) uint32_t sP[GP * N];
-    __shared__ unsigned s_fail[2], s_last[2];
+    __shared__ unsigned s_fail[2], s_last[2], s_half[2];
 
     const int tid = threadIdx.x;
     const int g = GP == 1 ? 0 : tid / Z;
@@ -229,6 +229,8 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
         s_fail[1] = 0;
         s_last[0] = 0;
         s_last[1] = 0;
+        s_half[0] = 0;
+        s_half[1] = 0;
     }
     /* staging: word v of pair q holds variable v of frames 2q (low lane) and
      * 2q+1 (high lane); all loads are issued before the conversions */
@@ -292,6 +294,7 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
     using L0 = std::integral_constant<int, 0>;
     using L1 = std::integral_constant<int, 1>;
     using LM = std::integral_constant<int, MB - 1>;
+    using LH = std::integral_constant<int, (MB - 1) / 2>;
     using LE = std::integral_constant<int, MB>;
     unsigned fmask = frame_fail(live ? rows_fail(L0{}, L1{}) & h2_lanes(live) : 0u, &s_last[0]);
     if (((1u << nf) - 1u) & ~fmask) {
@@ -306,6 +309,7 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
         if (tid == 0) {
             s_fail[slot] = 0;
             s_last[slot] = 0;
+            s_half[slot] = 0;
         }
         const uint32_t am = h2_lanes(act);     /* lanes still decoding; frozen lanes get mu = 0 */
         const uint2* wab = a.wab[t < a.wrows ? t : a.wrows - 1];
@@ -348,16 +352,19 @@ lms16_decode_kernel(const __grid_constant__ Lms16Args a)
             if constexpr (!LAST) __syncthreads();
         });
         /* stopping rule: a lane with a failing row in the last layer fails;
-         * the other active lanes check the remaining layers. The first vote
-         * is the last layer's barrier. */
+         * the other active lanes check the remaining layers in two halves,
+         * with a vote after each. The first vote is the last layer's barrier. */
         const unsigned lmask = frame_fail(act ? last_par & h2_lanes(act) : 0u, &s_last[slot]);
-        unsigned full = 0;
-        if (fmask & ~lmask) {
-            const unsigned chk = act & ~(lmask >> (2 * g)) & 3u;
-            full = frame_fail(chk ? rows_fail(L0{}, LM{}) & h2_lanes(chk) : 0u,
-                              &s_fail[slot]);
+        unsigned fm = lmask;
+        if (fmask & ~fm) {
+            const unsigned chk = act & ~(fm >> (2 * g)) & 3u;
+            fm |= frame_fail(chk ? rows_fail(L0{}, LH{}) & h2_lanes(chk) : 0u, &s_fail[slot]);
         }
-        fmask = lmask | full;
+        if (fmask & ~fm) {
+            const unsigned chk = act & ~(fm >> (2 * g)) & 3u;
+            fm |= frame_fail(chk ? rows_fail(LH{}, LM{}) & h2_lanes(chk) : 0u, &s_half[slot]);
+        }
+        fmask = fm;
         if (act & 1u) it0 = t + 1;
         if (act & 2u) it1 = t + 1;
         const unsigned nact = (fmask >> (2 * g)) & 3u;
