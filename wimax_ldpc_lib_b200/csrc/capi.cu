@@ -92,9 +92,10 @@ struct wldpc_decoder {
     unsigned* err = nullptr;   /* device error word */
     DevBuf llr, hard, status, bits;
     DevBuf pllr[kHostStages], phard[kHostStages], pstatus[kHostStages];
-    /* one frame per call: a device block [posterior 4n | hard n | status 4]
-     * and its pinned host image (+ the error word), so a call is one copy in,
-     * one launch and two copies out, none of them through pageable memory */
+    /* one frame per call: a device block [error word 4 | pad 12 | posterior 4n
+     * | hard n | status 4] and its pinned host image, so a call is one copy in
+     * (which also clears the error word), one launch and one copy out, none of
+     * them through pageable memory */
     DevBuf one;
     unsigned char* one_host = nullptr;
 };
@@ -228,14 +229,14 @@ int wldpc_decoder_destroy(wldpc_decoder* d)
 }
 
 static int decode_launch(wldpc_decoder* d, const float* llr, int8_t* hard, float* post, int32_t* status,
-                         size_t frames, cudaStream_t st)
+                         size_t frames, cudaStream_t st, unsigned* err = nullptr)
 {
     DecodeArgs a;
     a.llr = llr;
     a.hard = hard;
     a.post = post;
     a.status = status;
-    a.err = d->err;
+    a.err = err ? err : d->err;
     a.frames = (long long)frames;
     a.max_iter = (int)d->max_iter;
     a.wait_limit_us = d->wait_limit_us;
@@ -296,16 +297,19 @@ int wldpc_decoder_synchronize(wldpc_decoder* d)
 
 /* One frame (the reference's per-frame decode(float*)): the caller's buffers
  * are usually pageable, so the frame goes through the decoder's pinned block
- * by host memcpy and crosses PCIe in one copy each way. */
+ * by host memcpy and crosses PCIe in one copy each way. The block starts with
+ * the launch's own error word, which the copy in clears, so the copy out
+ * brings it back with the results. */
 static int decode_one_host(wldpc_decoder* d, float* rx, int8_t* decoded, int32_t* status_host)
 {
     const size_t n = (size_t)d->code.n;
-    const size_t block = 5 * n + 4;   /* 4n and 5n are multiples of 16 (n = 24 z, z a multiple of 4) */
+    const size_t head = 16;                 /* error word + pad: the posterior stays 16-byte aligned */
+    const size_t block = head + 5 * n + 4;  /* 4n and 5n are multiples of 16 (n = 24 z, z a multiple of 4) */
     int rc;
     if ((rc = d->one.reserve(block))) return rc;
     if (!d->one_host) {
         void* h = nullptr;
-        if (cudaHostAlloc(&h, block + 4, cudaHostAllocDefault) != cudaSuccess) {
+        if (cudaHostAlloc(&h, block, cudaHostAllocDefault) != cudaSuccess) {
             cudaGetLastError();
             return WLDPC_ERR_CUDA;
         }
@@ -313,28 +317,28 @@ static int decode_one_host(wldpc_decoder* d, float* rx, int8_t* decoded, int32_t
     }
     unsigned char* dev = (unsigned char*)d->one.p;
     unsigned char* host = d->one_host;
-    unsigned* err_host = (unsigned*)(host + block);
-    memcpy(host, rx, n * 4);
-    CU(cudaMemcpyAsync(dev, host, n * 4, cudaMemcpyHostToDevice, d->stream));
-    if ((rc = decode_launch(d, (const float*)dev, (int8_t*)(dev + 4 * n), (float*)dev, (int32_t*)(dev + 5 * n), 1,
-                            d->stream))) {
+    memset(host, 0, head);
+    memcpy(host + head, rx, n * 4);
+    CU(cudaMemcpyAsync(dev, host, head + n * 4, cudaMemcpyHostToDevice, d->stream));
+    unsigned char* dp = dev + head;
+    if ((rc = decode_launch(d, (const float*)dp, (int8_t*)(dp + 4 * n), (float*)dp, (int32_t*)(dp + 5 * n), 1,
+                            d->stream, (unsigned*)dev))) {
         cudaStreamSynchronize(d->stream);
         return rc;
     }
-    if (cudaMemcpyAsync(host, dev, block, cudaMemcpyDeviceToHost, d->stream) != cudaSuccess ||
-        cudaMemcpyAsync(err_host, d->err, 4, cudaMemcpyDeviceToHost, d->stream) != cudaSuccess) {
+    if (cudaMemcpyAsync(host, dev, block, cudaMemcpyDeviceToHost, d->stream) != cudaSuccess) {
         cudaStreamSynchronize(d->stream);
         cudaGetLastError();
         return WLDPC_ERR_CUDA;
     }
     CU(cudaStreamSynchronize(d->stream));
-    if (*err_host) {
-        CU(cudaMemset(d->err, 0, sizeof(unsigned)));
-        return WLDPC_ERR_TIMEOUT;
-    }
-    memcpy(rx, host, n * 4);
-    memcpy(decoded, host + 4 * n, n);
-    memcpy(status_host, host + 5 * n, 4);
+    unsigned errword = 0;
+    memcpy(&errword, host, 4);
+    if (errword) return WLDPC_ERR_TIMEOUT;
+    const unsigned char* hp = host + head;
+    memcpy(rx, hp, n * 4);
+    memcpy(decoded, hp + 4 * n, n);
+    memcpy(status_host, hp + 5 * n, 4);
     return WLDPC_OK;
 }
 
