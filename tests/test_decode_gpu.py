@@ -7,6 +7,7 @@ import pytest
 
 import inputs
 from cases import case_llr, expected_iters
+from test_learned_oracle import random_weights
 
 pytestmark = pytest.mark.gpu
 
@@ -82,6 +83,31 @@ def test_all_z_against_oracle(wl, cuda, oracle, rate):
         assert (post.view(np.uint32) == po.view(np.uint32)).all(), (rate, z)
         assert (hard == do).all(), (rate, z)
         assert ((status & 0xFFFF) == io).all() and (((status >> 16) & 1) == so).all(), (rate, z)
+
+
+@pytest.mark.parametrize("rate", range(6))
+def test_multi_frame_ctas_with_a_partial_last_cta(wl, cuda, oracle, rate):
+    """z not a multiple of 32 puts several frames in one CTA (their stopping
+    votes are per frame); 37 frames leave the last CTA partly empty, and every
+    third frame is a clean codeword (0 iterations) next to noisy ones that stop
+    at different iterations or run to the cap."""
+    for z in (24, 28, 36, 44, 52, 68, 76, 84, 92):
+        _, cw, llr = inputs.frames(oracle, rate, z, 37, inputs.SWEEP_EBNO[rate] - 0.5, seed=8100 + rate * 100 + z)
+        llr[::3] = np.where(cw[::3] != 0, 4.0, -4.0).astype(np.float32)
+        po, do, ro, io, so = oracle.decode(rate, z, llr, 10)
+        assert (io[::3] == 0).all() and (io > 0).any()
+        post, hard, status = run_device(wl, cuda, wl.Decoder(rate, z, 10), llr)
+        assert (post.view(np.uint32) == po.view(np.uint32)).all(), (rate, z)
+        assert (hard == do).all(), (rate, z)
+        assert ((status & 0xFFFF) == io).all() and (((status >> 16) & 1) == so).all(), (rate, z)
+        # the learned decoders' stopping votes on the same frames, against the oracle's restatements
+        w, _, _ = random_weights(oracle, rate, z, 8, 8200 + rate * 100 + z)
+        w[1] = np.abs(w[1])                      # in the binary16 decoder's range (b >= 0)
+        for prec, ref in ((wl.LMS_F32, oracle.learned_decode), (wl.LMS_F16X2, oracle.learned16_decode)):
+            po, do, io, so = ref(rate, z, 8, w, llr, cap=10)
+            post, hard, _, st = wl.LearnedDecoder(rate, z, 8, weights=w, cap=10, precision=prec).decode_host(llr)
+            assert (post.view(np.uint32) == po.view(np.uint32)).all(), (prec, rate, z)
+            assert (hard == do).all() and ((st & 0xFFFF) == io).all() and (((st >> 16) & 1) == so).all(), (prec, rate, z)
 
 
 @pytest.mark.parametrize("mode", [1, 2])
