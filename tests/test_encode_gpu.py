@@ -35,6 +35,32 @@ def test_encoder_large_batch_against_oracle(wl, cuda, oracle):
         assert (cw.cpu().numpy() == oracle.encode(rate, z, u)).all()
 
 
+@pytest.mark.parametrize("rate,z", [(0, 24), (1, 60), (3, 28), (3, 44), (5, 92), (2, 96)])
+def test_encoder_partial_warps_odd_bytes_and_unaligned_buffers(wl, cuda, oracle, rate, z):
+    """The (rate, z)-specialised encoder takes 32 frames per warp: 45 frames
+    leave a partial warp; bytes other than 0/1 must count as 1 and pass
+    through to the systematic part; rate 3/4 at z = 28, 44 moves 8-byte
+    chunks; buffers that are only 4-byte aligned take the generic kernel."""
+    torch = cuda
+    n, m, k = inputs.code_dims(rate, z)
+    frames = 45
+    u = inputs.info_bits(7000 + rate * 100 + z, frames, k)
+    r = inputs.raw(7001 + rate * 100 + z, frames * k).reshape(frames, k)
+    u = np.where(r % np.uint64(7) == 0, (r >> np.uint64(8)) % np.uint64(256), u).astype(np.uint8)
+    want = oracle.encode(rate, z, u)
+    enc = wl.Encoder(rate, z)
+    cw = torch.empty((frames, n), dtype=torch.uint8, device="cuda")
+    enc.encode_device(torch.from_numpy(u).cuda(), cw)
+    torch.cuda.synchronize()
+    assert (cw.cpu().numpy() == want).all()
+    ub = torch.zeros(frames * k + 16, dtype=torch.uint8, device="cuda")
+    cb = torch.zeros(frames * n + 16, dtype=torch.uint8, device="cuda")
+    ub[4:4 + frames * k] = torch.from_numpy(u.reshape(-1)).cuda()
+    enc.encode_device(ub[4:4 + frames * k].view(frames, k), cb[4:4 + frames * n].view(frames, n))
+    torch.cuda.synchronize()
+    assert (cb[4:4 + frames * n].view(frames, n).cpu().numpy() == want).all()
+
+
 @pytest.mark.parametrize("rate", [0, 1, 2, 3, 5])
 def test_framegen_matches_oracle(wl, cuda, oracle, rate):
     torch = cuda

@@ -335,10 +335,31 @@ cudaError_t launch_lfsr_bits(unsigned long long first_bit, long long nbits, uint
 
 /* ---------------------------------------------------------------- launchers */
 
+extern const EncLanesLaunch kEncLanes_r0[kNumZ];
+extern const EncLanesLaunch kEncLanes_r1[kNumZ];
+extern const EncLanesLaunch kEncLanes_r2[kNumZ];
+extern const EncLanesLaunch kEncLanes_r3[kNumZ];
+extern const EncLanesLaunch kEncLanes_r5[kNumZ];
+
+const EncLanesLaunch* enc_lanes_entry(int rate, int z)
+{
+    static const EncLanesLaunch* const tables[kRates] = {kEncLanes_r0, kEncLanes_r1, kEncLanes_r2,
+                                                         kEncLanes_r3, nullptr, kEncLanes_r5};
+    if (!valid_rate(rate) || !valid_z(z) || !tables[rate]) return nullptr;
+    return &tables[rate][z_index(z)];
+}
+
 cudaError_t launch_encode_bytes(const CodeDesc& c, const uint8_t* info, uint8_t* cw, long long frames,
                                 cudaStream_t st)
 {
     if (frames <= 0) return cudaSuccess;
+    const EncLanesLaunch* e = enc_lanes_entry(c.rate, c.z);
+    if (e && ((uintptr_t)info % e->align) == 0 && ((uintptr_t)cw % e->align) == 0) {
+        const long long frames_per_cta = e->threads;   /* one frame per thread */
+        e->kernel<<<(unsigned)((frames + frames_per_cta - 1) / frames_per_cta), e->threads, 0, st>>>(info, cw,
+                                                                                                   frames);
+        return cudaGetLastError();
+    }
     const long long blocks = (frames + kEncWarps - 1) / kEncWarps;
     encode_bytes_kernel<<<(unsigned)blocks, 32 * kEncWarps, 0, st>>>(c, info, cw, frames);
     return cudaGetLastError();

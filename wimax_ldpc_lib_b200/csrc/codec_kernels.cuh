@@ -35,6 +35,17 @@ struct NullspaceArgs {
 
 cudaError_t launch_framegen_nullspace(const CodeDesc& c, const FramegenArgs& a, const NullspaceArgs& ns,
                                       cudaStream_t st);
+/* encoder specialised on (rate, z), one frame per lane (encode_lanes.cuh);
+ * info and codeword must be aligned to `align` bytes */
+struct EncLanesLaunch {
+    void (*kernel)(const uint8_t*, uint8_t*, long long);
+    int align;
+    int threads;        /* per CTA: 32 frames per warp */
+};
+/* entry for (rate, z) or null (rate 3/4B has no encoder) */
+const EncLanesLaunch* enc_lanes_entry(int rate, int z);
+/* the encoder over a batch: the (rate, z)-specialised kernel when the
+ * buffers are aligned for it, else the generic one-warp-per-frame kernel */
 cudaError_t launch_encode_bytes(const CodeDesc& c, const uint8_t* info, uint8_t* cw, long long frames,
                                 cudaStream_t st);
 cudaError_t launch_framegen(const CodeDesc& c, const FramegenArgs& a, cudaStream_t st);

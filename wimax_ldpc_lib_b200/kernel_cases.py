@@ -8,7 +8,7 @@ for profilers (ncu: every launch below is one capture) and quick timing.
              (tdmp_decode_kernel), the learned decoder with its shipped
              weights (lms_decode_kernel) and the same weights in packed
              binary16 (lms16_decode_kernel), cap 10
-  encode     F rate 1/2 z = 96 info words (encode_bytes_kernel)
+  encode     F rate 1/2 z = 96 info words (encode_lanes_kernel)
 
   train      one Adam step of the learned decoder's training (rate 1/2,
              z = 96, F/16 frames generated on the device): framegen_kernel,
