@@ -139,6 +139,30 @@ def test_bits_adapter_and_syndrome(wl, cuda, oracle, golden_misc):
             assert dec.compute_syndrome(bits[f], True) == s["early"][f]
 
 
+@pytest.mark.parametrize("rate,z", [(0, 96), (4, 28), (5, 60), (1, 24), (3, 92), (2, 44)])
+def test_syndrome_batch_against_oracle(wl, cuda, oracle, rate, z):
+    """Batch compute_syndrome: 45 frames (a partial warp of the specialised
+    kernel) of codewords with 0 to a few hundred flipped bits; a third of the
+    frames carry bytes other than 0 and 1 (the reference XORs whole bytes, so
+    the kernel checks bit planes 1..7 of those frames too)."""
+    n, m, k = inputs.code_dims(rate, z)
+    frames = 45
+    cw = oracle.encode(rate, z, inputs.info_bits(6100 + z, frames, k)) if rate != 4 else np.zeros((frames, n), np.uint8)
+    bits = cw.astype(np.int8)
+    r = inputs.raw(6200 + rate * 100 + z, frames * n).reshape(frames, n)
+    for f in range(frames):
+        flips = (r[f] % np.uint64(max(1, 40 * f))) == 0 if f else np.zeros(n, bool)
+        bits[f, flips] ^= 1
+        if f % 3 == 1:
+            odd = (r[f] >> np.uint64(20)) % np.uint64(9) == 0
+            bits[f, odd] = ((r[f, odd] >> np.uint64(32)) % np.uint64(256)).astype(np.uint8).view(np.int8)
+    dec = wl.Decoder(rate, z, 10)
+    for early in (False, True):
+        want = oracle.syndrome(rate, z, bits, early)
+        assert (dec.syndrome_host(bits, early) == want).all(), (rate, z, early)
+    assert (want == 0).any() and (want == 1).any()
+
+
 def test_max_iter_zero_quirk(wl, cuda, oracle):
     llr = inputs.edge_llr("noise", 0, 48, 8, 5)
     dec = wl.Decoder(0, 48, 0)

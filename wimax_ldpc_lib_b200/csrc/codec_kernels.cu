@@ -1,12 +1,15 @@
 /*
- * Encoder, frame generation, syndrome and input-adapter kernels.
+ * Encoder, frame generation and input-adapter kernels, and the launchers of
+ * the (rate, z)-specialised encoder and compute_syndrome kernels
+ * (encode_lanes.cuh, syndrome_lanes.cuh).
  *
  *  encode_bytes_kernel  - ldpc_encoder::encode_data over a batch
- *                         (reference lib/ldpc_encoder.cc:50-105), one warp per frame
+ *                         (reference lib/ldpc_encoder.cc:50-105), one warp per
+ *                         frame, for buffers not aligned for encode_lanes_kernel
+ *                         and for rate 3/4B
  *  framegen_kernel      - seeded synthetic frames: Philox info bits, the same
  *                         encoder on packed words, BPSK bit*2-1 (reference
  *                         lib/BER_runner.cc:183), AWGN, LLR = 2y/sigma^2
- *  syndrome_kernel      - compute_syndrome (reference lib/ldpc_decoder.cc:67-104)
  *  bits_to_llr_kernel   - the int8 input adapter bit*2.0-1.0 (reference
  *                         lib/ldpc_decoder.cc:108-118)
  */
@@ -245,33 +248,6 @@ framegen_nullspace_kernel(CodeDesc c, FramegenArgs a, NullspaceArgs ns)
     if (a.llr) emit_llr(c, a, f, g, scale, sigma, lane, [&](int j) -> uint32_t { return C[j >> 5] >> (j & 31); });
 }
 
-/* One thread per expanded check row; rows of a frame are contiguous in
- * threadIdx.x. out[f] = number of failing rows, or 0/1 with early_exit. */
-__global__ void syndrome_kernel(CodeDesc c, const int8_t* __restrict__ bits, uint32_t* __restrict__ out,
-                                long long frames, int early_exit)
-{
-    const long long f = blockIdx.x;
-    if (f >= frames) return;
-    const int8_t* x = bits + f * c.n;
-    __shared__ uint32_t count;
-    if (threadIdx.x == 0) count = 0;
-    __syncthreads();
-    uint32_t local = 0;
-    for (int row = threadIdx.x; row < c.m; row += blockDim.x) {
-        const int i = row / c.z, r = row - i * c.z;
-        int8_t acc = 0;
-        for (int b = c.row_start[i]; b < c.row_start[i + 1]; b++) {
-            int t = r + c.shift[b];
-            t = t >= c.z ? t - c.z : t;
-            acc ^= x[c.col[b] * c.z + t];
-        }
-        local += acc != 0;
-    }
-    if (local) atomicAdd(&count, local);
-    __syncthreads();
-    if (threadIdx.x == 0) out[f] = early_exit ? (count != 0) : count;
-}
-
 __global__ void bits_to_llr_kernel(const int8_t* __restrict__ bits, float* __restrict__ llr, long long count)
 {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
@@ -382,11 +358,30 @@ cudaError_t launch_framegen_nullspace(const CodeDesc& c, const FramegenArgs& a, 
     return cudaGetLastError();
 }
 
+extern const SynLanesLaunch kSynLanes_r0[kNumZ];
+extern const SynLanesLaunch kSynLanes_r1[kNumZ];
+extern const SynLanesLaunch kSynLanes_r2[kNumZ];
+extern const SynLanesLaunch kSynLanes_r3[kNumZ];
+extern const SynLanesLaunch kSynLanes_r4[kNumZ];
+extern const SynLanesLaunch kSynLanes_r5[kNumZ];
+
+const SynLanesLaunch* syn_lanes_entry(int rate, int z)
+{
+    static const SynLanesLaunch* const tables[kRates] = {kSynLanes_r0, kSynLanes_r1, kSynLanes_r2,
+                                                         kSynLanes_r3, kSynLanes_r4, kSynLanes_r5};
+    if (!valid_rate(rate) || !valid_z(z)) return nullptr;
+    return &tables[rate][z_index(z)];
+}
+
 cudaError_t launch_syndrome(const CodeDesc& c, const int8_t* bits, uint32_t* out, long long frames,
                             int early_exit, cudaStream_t st)
 {
     if (frames <= 0) return cudaSuccess;
-    syndrome_kernel<<<(unsigned)frames, 256, 0, st>>>(c, bits, out, frames, early_exit);
+    const SynLanesLaunch* e = syn_lanes_entry(c.rate, c.z);
+    if (!e || ((uintptr_t)bits % 16) != 0 || ((uintptr_t)out % 4) != 0) return cudaErrorInvalidValue;
+    const long long frames_per_cta = e->threads;   /* one frame per thread */
+    e->kernel<<<(unsigned)((frames + frames_per_cta - 1) / frames_per_cta), e->threads, 0, st>>>(bits, out, frames,
+                                                                                               early_exit);
     return cudaGetLastError();
 }
 

@@ -44,11 +44,20 @@ struct EncLanesLaunch {
 };
 /* entry for (rate, z) or null (rate 3/4B has no encoder) */
 const EncLanesLaunch* enc_lanes_entry(int rate, int z);
+/* compute_syndrome specialised on (rate, z), one frame per lane
+ * (syndrome_lanes.cuh); the bytes must be 16-byte aligned */
+struct SynLanesLaunch {
+    void (*kernel)(const int8_t*, uint32_t*, long long, int);
+    int threads;        /* per CTA: 32 frames per warp */
+};
+const SynLanesLaunch* syn_lanes_entry(int rate, int z);
 /* the encoder over a batch: the (rate, z)-specialised kernel when the
  * buffers are aligned for it, else the generic one-warp-per-frame kernel */
 cudaError_t launch_encode_bytes(const CodeDesc& c, const uint8_t* info, uint8_t* cw, long long frames,
                                 cudaStream_t st);
 cudaError_t launch_framegen(const CodeDesc& c, const FramegenArgs& a, cudaStream_t st);
+/* compute_syndrome over a batch (syndrome_lanes.cuh); the bytes must be
+ * 16-byte aligned (the C ABI stages them in its own device buffers) */
 cudaError_t launch_syndrome(const CodeDesc& c, const int8_t* bits, uint32_t* out, long long frames,
                             int early_exit, cudaStream_t st);
 cudaError_t launch_bits_to_llr(const int8_t* bits, float* llr, long long count, cudaStream_t st);

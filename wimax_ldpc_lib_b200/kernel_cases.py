@@ -14,7 +14,7 @@ for profilers (ncu: every launch below is one capture) and quick timing.
              z = 96, F/16 frames generated on the device): framegen_kernel,
              lms_train_kernel, lms_reduce_adam_kernel
   syndrome   compute_syndrome over F host frames of rate 1/2 z = 96 hard bits
-             (syndrome_kernel, reference lib/ldpc_decoder.cc:67-104)
+             (syndrome_lanes_kernel, reference lib/ldpc_decoder.cc:67-104)
   bits       decode(int8_t*) over F host frames of +-1 hard bits with 50 flips
              (bits_to_llr_kernel, then the decoder; reference
              lib/ldpc_decoder.cc:108-118)
