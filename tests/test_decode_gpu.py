@@ -139,6 +139,22 @@ def test_bits_adapter_and_syndrome(wl, cuda, oracle, golden_misc):
             assert dec.compute_syndrome(bits[f], True) == s["early"][f]
 
 
+def test_decode_bits_batch_with_any_byte_values(wl, cuda, oracle):
+    """decode(int8_t*) over a batch: bytes b become LLRs 2b - 1 (reference
+    lib/ldpc_decoder.cc:108-118) for every int8 value, not only 0 and 1."""
+    rate, z, frames = 0, 48, 37
+    n, m, k = inputs.code_dims(rate, z)
+    bits = oracle.encode(rate, z, inputs.info_bits(6300, frames, k)).astype(np.int8)
+    r = inputs.raw(6301, frames * n).reshape(frames, n)
+    bits[(r % np.uint64(97)) == 0] ^= 1
+    odd = (r >> np.uint64(16)) % np.uint64(211) == 0
+    bits[odd] = ((r[odd] >> np.uint64(32)) % np.uint64(256)).astype(np.uint8).view(np.int8)
+    bits[0, :4] = [-128, 127, -1, 0]
+    d_ref, ret_ref, _ = oracle.decode_bits(rate, z, bits, 10)
+    d, ne = wl.Decoder(rate, z, 10).decode_bits_host(bits)
+    assert (d == d_ref).all() and (ne == ret_ref).all()
+
+
 @pytest.mark.parametrize("rate,z", [(0, 96), (4, 28), (5, 60), (1, 24), (3, 92), (2, 44)])
 def test_syndrome_batch_against_oracle(wl, cuda, oracle, rate, z):
     """Batch compute_syndrome: 45 frames (a partial warp of the specialised

@@ -248,11 +248,41 @@ framegen_nullspace_kernel(CodeDesc c, FramegenArgs a, NullspaceArgs ns)
     if (a.llr) emit_llr(c, a, f, g, scale, sigma, lane, [&](int j) -> uint32_t { return C[j >> 5] >> (j & 31); });
 }
 
+/* bit*2.0-1.0 with the reference's double literals (reference
+ * lib/ldpc_decoder.cc:108-118): for an int8 bit the result 2b - 1 is an odd
+ * integer in [-257, 253], which a float holds exactly, so integer arithmetic
+ * and an exact conversion give the float the double computation rounds to.
+ * The conversion adds 2b - 1 to the mantissa of 1.5 * 2^23 (whose unit in
+ * the last place is 1) and subtracts 1.5 * 2^23 again; both steps are exact
+ * for |2b - 1| < 2^22. */
+__device__ __forceinline__ float bit_to_llr(int b)
+{
+    return __int_as_float(0x4B3FFFFF + 2 * b) - 12582912.0f;
+}
+
+/* 4 bytes in and one float4 out per thread and step where the bytes are
+ * 4-byte and the LLRs 16-byte aligned (both coalesced over a warp: 128 bytes
+ * in, 512 out), the loads of four steps issued before any is used; a scalar
+ * loop takes the rest */
 __global__ void bits_to_llr_kernel(const int8_t* __restrict__ bits, float* __restrict__ llr, long long count)
 {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
-         i += (long long)gridDim.x * blockDim.x)
-        llr[i] = (float)__dadd_rn(__dmul_rn((double)bits[i], 2.0), -1.0);
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long nvec = ((uintptr_t)bits % 4 == 0 && (uintptr_t)llr % 16 == 0) ? count / 4 : 0;
+    const unsigned int* in = reinterpret_cast<const unsigned int*>(bits);
+    float4* out = reinterpret_cast<float4*>(llr);
+    for (long long v = t0; v < nvec; v += 4 * stride) {
+        uint32_t x[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) x[u] = v + u * stride < nvec ? __ldcs(in + v + u * stride) : 0u;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (v + u * stride < nvec)   /* byte j sign-extended: (int)(x << (24 - 8j)) >> 24 */
+                __stcs(out + v + u * stride,
+                       make_float4(bit_to_llr((int)(x[u] << 24) >> 24), bit_to_llr((int)(x[u] << 16) >> 24),
+                                   bit_to_llr((int)(x[u] << 8) >> 24), bit_to_llr((int)x[u] >> 24)));
+    }
+    for (long long i = nvec * 4 + t0; i < count; i += stride) llr[i] = bit_to_llr(bits[i]);
 }
 
 /* The reference BER_runner's info-bit stream (reference lib/BER_runner.cc:35-41,
@@ -388,7 +418,7 @@ cudaError_t launch_syndrome(const CodeDesc& c, const int8_t* bits, uint32_t* out
 cudaError_t launch_bits_to_llr(const int8_t* bits, float* llr, long long count, cudaStream_t st)
 {
     if (count <= 0) return cudaSuccess;
-    long long blocks = (count + 255) / 256;
+    long long blocks = (count / 4 + 255) / 256 + 1;
     if (blocks > 148 * 32) blocks = 148 * 32;
     bits_to_llr_kernel<<<(unsigned)blocks, 256, 0, st>>>(bits, llr, count);
     return cudaGetLastError();
