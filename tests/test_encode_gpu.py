@@ -90,3 +90,8 @@ def test_lfsr_stream_matches_reference_generator(wl, cuda, oracle):
         wl.lfsr_bits_device(first, out)
         torch.cuda.synchronize()
         assert (out.cpu().numpy() == ref[first:first + 5000]).all(), first
+        buf = torch.zeros(5008, dtype=torch.uint8, device="cuda")   # output not 16-byte aligned
+        wl.lfsr_bits_device(first, buf[3:3 + 4999])
+        torch.cuda.synchronize()
+        assert (buf[3:3 + 4999].cpu().numpy() == ref[first:first + 4999]).all(), first
+        assert not buf[:3].cpu().numpy().any() and not buf[3 + 4999:].cpu().numpy().any()

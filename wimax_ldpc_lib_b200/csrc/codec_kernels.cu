@@ -293,10 +293,33 @@ __global__ void bits_to_llr_kernel(const int8_t* __restrict__ bits, float* __res
 constexpr int kLfsrPeriod = 115200;
 __device__ uint32_t g_lfsr_period[kLfsrPeriod / 32];
 
+/* 16 bits of the period from bit p on (p < kLfsrPeriod), wrapping at the
+ * period's end, which falls on a word boundary */
+__device__ __forceinline__ uint32_t lfsr_bits16(unsigned p)
+{
+    constexpr unsigned kWords = kLfsrPeriod / 32;
+    const unsigned w = p >> 5;
+    const uint32_t lo = g_lfsr_period[w], hi = g_lfsr_period[w + 1 == kWords ? 0 : w + 1];
+    return __funnelshift_r(lo, hi, p & 31) & 0xFFFFu;
+}
+
+/* Output bytes 0/1. Where out is 16-byte aligned, a thread writes 16 bytes
+ * per step (one modulo per 16 bits, the bits expanded to bytes by
+ * multiplication, one 16-byte store); a scalar loop takes the rest. */
 __global__ void lfsr_bits_kernel(unsigned long long first_bit, long long nbits, uint8_t* __restrict__ out)
 {
-    for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < nbits;
-         j += (long long)gridDim.x * blockDim.x) {
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long nvec = ((uintptr_t)out % 16 == 0) ? nbits / 16 : 0;
+    for (long long g = t0; g < nvec; g += stride) {
+        const unsigned p = (unsigned)((first_bit + 16ull * (unsigned long long)g) % kLfsrPeriod);
+        const uint32_t b = lfsr_bits16(p);
+        __stcs(reinterpret_cast<uint4*>(out) + g,
+               make_uint4(((b & 0xFu) * 0x00204081u) & 0x01010101u, (((b >> 4) & 0xFu) * 0x00204081u) & 0x01010101u,
+                          (((b >> 8) & 0xFu) * 0x00204081u) & 0x01010101u,
+                          (((b >> 12) & 0xFu) * 0x00204081u) & 0x01010101u));
+    }
+    for (long long j = nvec * 16 + t0; j < nbits; j += stride) {
         const unsigned p = (unsigned)((first_bit + (unsigned long long)j) % kLfsrPeriod);
         out[j] = (uint8_t)((g_lfsr_period[p >> 5] >> (p & 31)) & 1u);
     }
@@ -333,7 +356,7 @@ cudaError_t upload_lfsr_period(const uint32_t* words)
 cudaError_t launch_lfsr_bits(unsigned long long first_bit, long long nbits, uint8_t* out, cudaStream_t st)
 {
     if (nbits <= 0) return cudaSuccess;
-    long long blocks = (nbits + 255) / 256;
+    long long blocks = (nbits / 16 + 255) / 256 + 1;
     if (blocks > 148 * 16) blocks = 148 * 16;
     lfsr_bits_kernel<<<(unsigned)blocks, 256, 0, st>>>(first_bit, nbits, out);
     return cudaGetLastError();
