@@ -7,7 +7,7 @@
  * and counts the rows whose XOR is non-zero (or returns 1 at the first one
  * with early exit; the count and the early-exit answer differ only in that
  * the latter is min(count, 1)). A byte XOR is the XOR of its 8 bit planes, so
- * a row fails when any plane has odd parity. A warp encodes 32 frames:
+ * a row fails when any plane has odd parity. A warp checks 32 frames:
  *  A. per frame, the whole warp reads the n bytes in 16-byte chunks,
  *     coalesced, packs bit 0 of every byte into the frame's row of shared
  *     memory and notes whether any byte has another bit set;
