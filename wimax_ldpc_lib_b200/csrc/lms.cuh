@@ -227,6 +227,8 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
         /* parity of the last layer's row from the posteriors it writes: no
          * later layer changes them in this iteration, so they are final */
         bool last_odd = false;
+        /* this iteration's (a, b) pairs: the same address in every thread */
+        const float2* const wab = a.wab[t < a.wrows ? t : a.wrows - 1];
         static_for<MB>([&](auto I) {
             constexpr int d = layer_degree(R, I);
             constexpr int b0 = block_index(R, I, 0);
@@ -246,8 +248,6 @@ lms_decode_kernel(const __grid_constant__ LmsArgs a)
                 /* positive LLR = bit 1: the extrinsic sign flips on odd-degree rows */
                 const uint32_t fb = (sgn ^ ((uint32_t)(d & 1) << 31)) & 0x80000000u;
                 const uint32_t fbo = fb | 0x3f800000u;   /* with sign(L_e): +-1.0 */
-                const int wr = t < a.wrows ? t : a.wrows - 1;
-                const float2* wab = a.wab[wr];
                 static_for<d>([&](auto E_) {
                     constexpr int e = decltype(E_)::value;
                     const float l = L[e];
